@@ -1,0 +1,225 @@
+/*
+ * orchard_b200.h -- C ABI of the B200 (sm_100a) projection time step.
+ *
+ * Drop-in boundary for the CPU path of Orchard Flow (zfifteen/solver).  The
+ * reference has no FFI layer; its seams are C++ free functions, and each entry
+ * point below replaces one of them (cited as file:line in the reference).  The
+ * C++ mirror of those functions (solver_b200/host/orchard/...) and the Python
+ * binding (solver_b200/_capi.py) are thin layers over this header.
+ *
+ * Conventions
+ *  - All arrays are the reference's padded MAC storage, double precision,
+ *    one ghost layer, index i + sx*(j + sy*k), i unit-stride
+ *    (core/field_layout.hpp:178-183).  A cell field has storage
+ *    (nx+2, ny+2, nz+2); the face field normal to axis a has one more entry
+ *    along a (core/field_layout.hpp:75-86).
+ *  - Host arrays are borrowed for the duration of a call only.  Calls are
+ *    synchronous: they return after results and diagnostics are on the host.
+ *  - One context per host thread; a context owns one CUDA stream and all
+ *    device memory for its grid (state, scratch, multigrid hierarchy).
+ *  - Every entry point returns an of_status; of_last_error() gives the text of
+ *    the last failure on the calling thread, worded as the reference's
+ *    exceptions so that the C++ layer can rethrow them unchanged.
+ *  - There is no CPU fallback: a missing or unusable GPU is an error.
+ */
+#ifndef ORCHARD_B200_H
+#define ORCHARD_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OF_ABI_VERSION 1
+
+typedef enum {
+  OF_OK = 0,
+  OF_INVALID_ARGUMENT = 1, /* std::invalid_argument in the reference */
+  OF_RUNTIME_ERROR = 2,    /* std::runtime_error: zero pivot, singular coarse matrix */
+  OF_NOT_CONVERGED = 3,    /* require_converged_pressure_projection (solver/projection.cpp:1133) */
+  OF_NONFINITE = 4,        /* "... solve produced a non-finite state" (solver/taylor_green.cpp:614) */
+  OF_CUDA_ERROR = 5,
+  OF_TIMEOUT = 6           /* a device-side wait gave up (never expected) */
+} of_status;
+
+/* Grid (core/grid.hpp:57-87); ghost_layers is always 1. */
+typedef struct {
+  int nx, ny, nz;
+  double dx, dy, dz;
+} of_grid;
+
+/* PhysicalBoundaryType (bc/boundary_conditions.hpp:10-16) */
+enum { OF_NO_SLIP_WALL = 0, OF_PRESCRIBED_VELOCITY = 1, OF_SYMMETRY = 2, OF_FIXED_PRESSURE = 3,
+       OF_PERIODIC = 4 };
+/* PressureBoundaryType (bc/boundary_conditions.hpp:18-22) */
+enum { OF_P_NEUMANN = 0, OF_P_DIRICHLET = 1, OF_P_PERIODIC = 2 };
+
+/* BoundaryCondition (bc/boundary_conditions.hpp:24-29) */
+typedef struct {
+  int type;
+  double velocity[3];
+  double pressure;
+  double pressure_gradient;
+} of_face_bc;
+
+/* BoundaryConditionSet; faces x_min, x_max, y_min, y_max, z_min, z_max. */
+typedef struct {
+  of_face_bc faces[6];
+} of_bc;
+
+/* PressureBoundaryCondition / PressureBoundarySet (bc/boundary_conditions.hpp:46-62) */
+typedef struct {
+  int type;
+  double value;
+  double gradient;
+} of_pface_bc;
+
+typedef struct {
+  of_pface_bc faces[6];
+} of_pbc;
+
+/* PoissonSolveDiagnostics (solver/projection.hpp:22-39); the four label
+ * strings ("mgpcg", "geometric_multigrid", "v_cycle", "damped_jacobi") and
+ * the residual history are supplied separately. */
+typedef struct {
+  int iterations;
+  double initial_residual_l2;
+  double final_residual_l2;
+  double relative_residual;
+  double removed_rhs_mean;
+  int multigrid_levels;
+  int coarse_unknowns;
+  int pre_smoothing_steps;
+  int post_smoothing_steps;
+  int converged;
+  int zero_mean_enforced;
+} of_poisson_diag;
+
+/* ProjectionDiagnostics (solver/projection.hpp:41-47) */
+typedef struct {
+  double rhs_l2;
+  double divergence_l2_before;
+  double divergence_l2_after;
+  double pressure_mean;
+  of_poisson_diag pressure_solve;
+} of_projection_diag;
+
+/* TaylorGreenStepMetrics (solver/taylor_green.hpp:32-42); the cavity's
+ * SimulationStepMetrics (solver/lid_driven_cavity.hpp:27-36) is the same
+ * without max_divergence_l2. */
+typedef struct {
+  int step;
+  double time;
+  double dt;
+  double max_cfl;
+  double max_velocity_change;
+  double divergence_l2;
+  double max_divergence_l2;
+  int pressure_iterations;
+  double pressure_relative_residual;
+} of_step_metrics;
+
+/* Arithmetic of the pressure solve.  OF_FP64 follows the reference; OF_MIXED
+ * runs the multigrid V-cycle in FP32 storage and arithmetic inside the FP64
+ * conjugate-gradient loop (residual, search direction, dot products, mean
+ * removal and the coarsest-grid solve stay FP64). */
+enum { OF_FP64 = 0, OF_MIXED = 1 };
+
+/* Predictor factorisation-correction variant: the Taylor-Green form
+ * (solver/taylor_green.cpp:196-225, 3D terms when nz > 1) or the cavity's 2D
+ * form (solver/lid_driven_cavity.cpp:219-252). */
+enum { OF_CORRECTION_TAYLOR_GREEN = 0, OF_CORRECTION_CAVITY = 1 };
+
+/* Parameters of one projection time step (the locals of
+ * run_taylor_green_steps, solver/taylor_green.cpp:556-564, and of
+ * advance_lid_driven_cavity_impl, solver/lid_driven_cavity.cpp:538-547). */
+typedef struct {
+  double viscosity;
+  double dt;
+  double density;
+  int poisson_max_iterations;
+  double poisson_tolerance;
+  int correction_variant;    /* OF_CORRECTION_* */
+  int track_max_divergence;  /* 1: update max_divergence_l2 (Taylor-Green) */
+  const char* solver_name;   /* "Taylor-Green" / "lid-driven cavity" for messages */
+} of_step_params;
+
+typedef struct of_ctx of_ctx;
+
+/* ---- library / context ------------------------------------------------- */
+
+int of_abi_version(void);
+/* Text of the last failure on this thread (empty if none). */
+const char* of_last_error(void);
+
+/* Creates a context for one grid and velocity boundary set on `device`
+ * (a CUDA ordinal).  Validates the grid like Grid's constructor
+ * (core/grid.hpp:76-86) and the pairing of periodic faces. */
+of_status of_create(const of_grid* grid, const of_bc* bc, int device, of_ctx** out);
+of_status of_destroy(of_ctx* ctx);
+of_status of_set_precision(of_ctx* ctx, int precision);
+/* Bytes of device memory the context holds. */
+of_status of_device_bytes(of_ctx* ctx, size_t* bytes);
+
+/* ---- operator entry points (host buffers) ------------------------------- */
+
+/* compute_advection_term, TVD/van Leer (solver/momentum_terms.hpp:36-38,
+ * solver/momentum_terms.cpp:307-314).  Writes the active entries of a*;
+ * their ghost entries are left as passed in. */
+of_status of_compute_advection_term(of_ctx* ctx, const double* u, const double* v,
+                                    const double* w, double* au, double* av, double* aw);
+
+/* solve_predictor_adi (solver/projection.hpp:49-52, solver/projection.cpp:1028-1047). */
+of_status of_solve_predictor_adi(of_ctx* ctx, double alpha, const double* rhs_u,
+                                 const double* rhs_v, const double* rhs_w, double* pred_u,
+                                 double* pred_v, double* pred_w, int* line_solves);
+
+/* linsolve::solve_pressure_poisson (linsolve/poisson_solver.hpp:34-37,
+ * linsolve/poisson_solver.cpp:678-809).  `pressure` is in/out (its active
+ * entries are the initial guess).  `history` receives up to history_cap
+ * residual norms (may be NULL). */
+of_status of_solve_pressure_poisson(of_ctx* ctx, const of_pbc* pbc, int max_iterations,
+                                    double tolerance, const double* rhs, double* pressure,
+                                    of_poisson_diag* diag, double* history, int history_cap);
+
+/* project_velocity (solver/projection.hpp:65-70, solver/projection.cpp:1097-1131).
+ * pressure_correction is in/out; pressure_rhs may be NULL. */
+of_status of_project_velocity(of_ctx* ctx, double dt, double density, int max_iterations,
+                              double tolerance, const double* pred_u, const double* pred_v,
+                              const double* pred_w, double* pressure_correction,
+                              double* corr_u, double* corr_v, double* corr_w,
+                              double* pressure_rhs, of_projection_diag* diag);
+
+/* ---- resident state (run_taylor_green_steps / run_lid_driven_cavity_steps) */
+
+/* Copies a TaylorGreenState / LidDrivenCavityState (solver/taylor_green.hpp:44-57)
+ * to the device.  adv_* is the AB2 history (advection_previous). */
+of_status of_state_upload(of_ctx* ctx, const double* u, const double* v, const double* w,
+                          const double* adv_u, const double* adv_v, const double* adv_w,
+                          const double* p_total, int has_previous_advection,
+                          const of_step_metrics* metrics);
+of_status of_state_download(of_ctx* ctx, double* u, double* v, double* w, double* adv_u,
+                            double* adv_v, double* adv_w, double* p_total,
+                            int* has_previous_advection, of_step_metrics* metrics);
+
+/* Taylor-Green initial state on the device (solver/taylor_green.cpp:335-395)
+ * for the context's grid.  mode 0: the reference's phase; mode 1: the same
+ * flow shifted by (pi/2, pi/2): u = sin x cos y [cos z],
+ * v = -cos x sin y [cos z], p = +1/4 (cos 2x + cos 2y) [2D] or
+ * +1/16 (cos 2x + cos 2y)(cos 2z + 2) [3D]. */
+of_status of_tg_init(of_ctx* ctx, double viscosity, double dt, int mode);
+
+/* Runs `steps` projection steps on the resident state: the loop body of
+ * run_taylor_green_steps (solver/taylor_green.cpp:577-633) and of
+ * advance_lid_driven_cavity_impl (solver/lid_driven_cavity.cpp:562-623).
+ * Fails with OF_NOT_CONVERGED / OF_NONFINITE at the step where the
+ * reference throws; the state then holds the last completed step. */
+of_status of_run_steps(of_ctx* ctx, const of_step_params* params, int steps,
+                       of_step_metrics* metrics);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ORCHARD_B200_H */

@@ -1,0 +1,137 @@
+// Host-side launchers of the B200 projection-step kernels.  Every launcher
+// enqueues on the given stream and returns immediately; the context code
+// (context.cu) sequences them into the reference's step.
+#pragma once
+
+#include "common.cuh"
+
+namespace ofb {
+
+// Device scalars shared by the pressure solve and the step diagnostics.  All
+// reductions land here; the host reads the block back once per iteration or
+// step.
+struct SolveScalars {
+  // pressure solve (linsolve/poisson_solver.cpp:678-809)
+  double sb, sx, sr, sp, sap, sz;  // pending mean shifts of b, x, r, p, Ap, z
+  double rz, pap, alpha, beta;
+  double sum_r;                    // sum of the stored residual
+  double r0, rnorm, rel;
+  double removed_rhs_mean;
+  double pressure_mean;
+  int iterations;
+  int converged;
+  int stop;                        // |p.Ap| < 1e-30 (linsolve/poisson_solver.cpp:757)
+  int zero_mean;
+  int n;                           // fine unknowns
+  double tol;
+  // projection / step diagnostics (solver/projection.cpp:1097-1131)
+  double div_before_l2, div_after_l2, rhs_l2;
+  double max_cfl, max_dv;
+  int nonfinite;
+};
+
+// Per-level mean shifts of the V-cycle vectors.
+struct LevelScalars {
+  double sb;  // rhs
+  double sa;  // smoother output a
+  double sx;  // smoother output b (the level's correction)
+  double sum_x;
+};
+
+// ---- boundary conditions (bc.cu) ----
+// apply_velocity_boundary_conditions (solver/projection.cpp:966-971) on three
+// face fields in place.
+void launch_velocity_bc(const Grid& g, const VBC& bc, double* u, double* v, double* w,
+                        cudaStream_t s);
+// Same on a single component (solve_component_adi's per-component calls).
+void launch_component_bc(const Grid& g, const VBC& bc, int comp, double* f, cudaStream_t s);
+// apply_total_pressure_boundary_conditions (solver/projection.cpp:986-1026) with
+// the wall-normal source nu * Laplacian(velocity) evaluated at the wall faces.
+void launch_total_pressure_bc(const Grid& g, const VBC& bc, double nu, const double* u,
+                              const double* v, const double* w, double* p, cudaStream_t s);
+
+// ---- momentum (momentum.cu) ----
+struct PredictorArgs {
+  Grid g;
+  const double* cur[3];   // current velocity (ghosts filled)
+  const double* p;        // total pressure (ghosts filled)
+  const double* prev[3];  // previous advection (AB2 history), may be unused
+  double* adv[3];         // out: advection at this step
+  double* rhs[3];         // out: predictor rhs (active entries)
+  double nu, dt, alpha;
+  int has_prev;
+  int variant;            // 0 Taylor-Green, 1 cavity
+};
+void launch_predictor_rhs(const PredictorArgs& a, cudaStream_t s);
+void launch_advection(const Grid& g, const double* u, const double* v, const double* w,
+                      double* au, double* av, double* aw, cudaStream_t s);
+void launch_tg_init(const Grid& g, int mode, double* u, double* v, double* w, double* p,
+                    cudaStream_t s);
+
+// ---- ADI (adi.cu) ----
+struct AdiPlan;  // per-(component, axis) Thomas coefficients, built on the host
+AdiPlan* adi_plan_create(const Grid& g, const VBC& bc, double alpha);
+void adi_plan_destroy(AdiPlan* p);
+// One sweep of solve_component_adi (solver/projection.cpp:868-888): reads the
+// active lines of `in`, writes the solved lines of `out`.
+void launch_adi_sweep(const AdiPlan* p, int comp, int axis, const double* in, double* out,
+                      cudaStream_t s);
+int adi_line_count(const AdiPlan* p, int comp, int axis);
+bool adi_axis_active(const AdiPlan* p, int comp, int axis);
+
+// ---- projection (projection.cu) ----
+// Divergence of the predicted velocity -> pressure rhs (rho/dt) div (padded,
+// active entries) and the compact system rhs b = -rhs - source
+// (solver/projection.cpp:1049-1064, linsolve/poisson_solver.cpp:701-705).
+void launch_divergence_rhs(const Grid& g, const PBC& pbc, const double* u, const double* v,
+                           const double* w, double scale, double* rhs_padded, double* b,
+                           SolveScalars* sc, RedBuf rb, cudaStream_t s);
+// System rhs from a caller-provided padded rhs (standalone Poisson solve).
+void launch_rhs_to_system(const Grid& g, const PBC& pbc, const double* rhs_padded, double* b,
+                          SolveScalars* sc, RedBuf rb, cudaStream_t s);
+// Compact initial guess from the padded pressure; sum -> sx.
+void launch_pressure_to_compact(const Grid& g, const double* p_padded, double* x,
+                                SolveScalars* sc, int zm, RedBuf rb, cudaStream_t s);
+// correct_velocity (solver/projection.cpp:1066-1095) active faces, and the
+// max |corrected - previous| reduction when prev != nullptr.
+void launch_correct_velocity(const Grid& g, const PBC& pbc, const double* x,
+                             const SolveScalars* sc, const double* pu, const double* pv,
+                             const double* pw, double scale, double* cu, double* cv, double* cw,
+                             const double* prev_u, const double* prev_v, const double* prev_w,
+                             SolveScalars* sc_out, RedBuf rb, cudaStream_t s);
+// Post-correction cell pass: divergence after, pressure mean, optional write of
+// the padded pressure correction, optional total-pressure update and CFL.
+struct CellPassArgs {
+  Grid g;
+  const double* u;
+  const double* v;
+  const double* w;
+  const double* x;           // compact pressure correction (shift sc->sx)
+  double* phi_padded;        // out (active), may be null
+  double* p_total;           // in/out, may be null
+  const double* rhs_padded;  // pressure rhs for the total-pressure update
+  double p_rhs_scale;        // -0.5 nu dt
+  double dt;                 // for the CFL diagnostic (0: skip)
+};
+void launch_cell_pass(const CellPassArgs& a, SolveScalars* sc, RedBuf rb, cudaStream_t s);
+
+// ---- Poisson (poisson.cu) ----
+struct PoissonPlan;  // hierarchy, coarse factorisation, work vectors
+PoissonPlan* poisson_plan_create(const Grid& g, const PBC& pbc, int precision);
+void poisson_plan_destroy(PoissonPlan* p);
+int poisson_levels(const PoissonPlan* p);
+int poisson_coarse_unknowns(const PoissonPlan* p);
+size_t poisson_device_bytes(const PoissonPlan* p);
+double* poisson_b(PoissonPlan* p);  // compact system rhs
+double* poisson_x(PoissonPlan* p);  // compact solution
+// Runs the MG-PCG loop on b (with shift sc->sb) and x (shift sc->sx).  Returns
+// after the device scalars hold the final diagnostics.  `history` (host) gets
+// the residual norms when non-null.
+void poisson_solve(PoissonPlan* p, int max_iterations, double tolerance, SolveScalars* sc_dev,
+                   SolveScalars* sc_host, RedBuf rb, cudaStream_t s, double* history,
+                   int history_cap);
+// Writes x - sx into the active entries of a padded pressure field.
+void launch_compact_to_pressure(const Grid& g, const double* x, const SolveScalars* sc,
+                                double* p_padded, cudaStream_t s);
+
+}  // namespace ofb

@@ -1,0 +1,856 @@
+// Multigrid-preconditioned CG for the pressure Poisson problem
+// (linsolve/poisson_solver.cpp:678-809) on compact, ghost-free vectors.
+//
+// Algorithm: the reference's exactly -- PCG on A = -Lap_h with BC-aware
+// neighbours (:195-269), one V(2,2) cycle per iteration with damped Jacobi
+// (omega = 2/3), 2x2x2 cell-average restriction, piecewise-constant
+// prolongation and a dense partially-pivoted Gaussian elimination on the
+// coarsest grid, and the zero-mean projection on singular (periodic /
+// all-Neumann) problems after every update.
+//
+// B200 form: each vector update is one kernel that also produces the sums the
+// next step needs (deterministic two-stage reduction, common.cuh).  A mean
+// removal is never a separate pass: the kernel that produces a vector records
+// its mean as a pending shift, and every consumer subtracts the shift as it
+// loads the vector -- the same arithmetic as the reference's
+// subtract_active_mean, one kernel later.  The Jacobi diagonal is a 64-entry
+// table per level (it only depends on whether a cell touches a boundary), the
+// V-cycle's residual is restricted on the fly (never stored) and the
+// prolongation is folded into the first post-smoothing sweep.  The V-cycle
+// storage type T is double (OF_FP64) or float (OF_MIXED: FP32 storage and
+// arithmetic inside the FP64 CG loop).
+#include "kernels.hpp"
+
+#include <cmath>
+#include <cstring>
+#include <type_traits>
+#include <vector>
+
+namespace ofb {
+
+namespace {
+
+constexpr double kSmallNumber = 1.0e-30;
+constexpr double kOmega = 2.0 / 3.0;
+constexpr int kMaxCoarse = 1024;
+
+struct OpInfo {
+  CLay L;
+  double inv2[3];  // 1 / h^2
+  int periodic[3];
+  int dir_lo[3], dir_hi[3];  // homogeneous Dirichlet (else Neumann) at each end
+  const double* invd;        // 64-entry inverse-diagonal table
+};
+
+__device__ __forceinline__ int axis_class(int c, int n) {
+  return n == 1 ? 3 : (c == 0 ? 1 : (c == n - 1 ? 2 : 0));
+}
+
+__device__ __forceinline__ double inv_diag(const OpInfo& o, int i, int j, int k) {
+  const int t = axis_class(i, o.L.nx) + 4 * axis_class(j, o.L.ny) + 16 * axis_class(k, o.L.nz);
+  return __ldg(&o.invd[t]);
+}
+
+// apply_poisson_operator at (i, j, k) with homogeneous boundary rules
+// (neighbor_value, linsolve/poisson_solver.cpp:195-242): periodic wrap,
+// Neumann ghost = centre, Dirichlet ghost = -centre.  val(i, j, k) returns the
+// operand at an in-range cell.
+template <typename A, typename F>
+__device__ __forceinline__ A apply_op(const OpInfo& o, int i, int j, int k, F val, A& center) {
+  const CLay& L = o.L;
+  const A c = val(i, j, k);
+  center = c;
+  A l, r, d, u, b, f;
+  if(i > 0) l = val(i - 1, j, k);
+  else l = o.periodic[0] ? val(L.nx - 1, j, k) : (o.dir_lo[0] ? -c : c);
+  if(i < L.nx - 1) r = val(i + 1, j, k);
+  else r = o.periodic[0] ? val(0, j, k) : (o.dir_hi[0] ? -c : c);
+  if(j > 0) d = val(i, j - 1, k);
+  else d = o.periodic[1] ? val(i, L.ny - 1, k) : (o.dir_lo[1] ? -c : c);
+  if(j < L.ny - 1) u = val(i, j + 1, k);
+  else u = o.periodic[1] ? val(i, 0, k) : (o.dir_hi[1] ? -c : c);
+  if(k > 0) b = val(i, j, k - 1);
+  else b = o.periodic[2] ? val(i, j, L.nz - 1) : (o.dir_lo[2] ? -c : c);
+  if(k < L.nz - 1) f = val(i, j, k + 1);
+  else f = o.periodic[2] ? val(i, j, 0) : (o.dir_hi[2] ? -c : c);
+  const A two_c = A(2) * c;
+  return -(r - two_c + l) * A(o.inv2[0]) - (u - two_c + d) * A(o.inv2[1]) -
+         (f - two_c + b) * A(o.inv2[2]);
+}
+
+template <int K>
+__device__ __forceinline__ void zero(double (&v)[K]) {
+#pragma unroll
+  for(int q = 0; q < K; ++q) v[q] = 0.0;
+}
+
+#define STENCIL_PROLOGUE(L)                                 \
+  const int i = blockIdx.x * kTX + threadIdx.x;             \
+  const int j = blockIdx.y * kTY + threadIdx.y;             \
+  const bool valid = i < (L).nx && j < (L).ny;              \
+  const int k0 = blockIdx.z * kchunk;                       \
+  const int k1 = min(k0 + kchunk, (L).nz);
+
+// ---------------------------------------------------------------------------
+// V-cycle kernels.  Level vectors are T; shifts and scalars are double.
+// ---------------------------------------------------------------------------
+
+// Pre-smoothing sweep 1 from a zero correction: a = omega (b - sb) / D.
+template <typename T, typename B>
+__global__ void __launch_bounds__(kTX* kTY)
+    k_smooth_first(OpInfo o, const B* __restrict__ b, const double* sb_ptr, T* __restrict__ a,
+                   LevelScalars* ls, int zm, int kchunk, RedBuf rb) {
+  STENCIL_PROLOGUE(o.L)
+  using A = T;
+  const double sb = *sb_ptr;
+  double acc[1];
+  zero(acc);
+  if(valid) {
+    for(int k = k0; k < k1; ++k) {
+      const int q = o.L.idx(i, j, k);
+      const A v = A(kOmega) * A(double(b[q]) - sb) * A(inv_diag(o, i, j, k));
+      a[q] = T(v);
+      acc[0] += double(v);
+    }
+  }
+  const bool mx[1] = {false};
+  const int n = o.L.count();
+  reduce_finish<1>(acc, mx, rb, [=](const Sums<1>& s) { ls->sa = zm ? s.v[0] / n : 0.0; });
+}
+
+// Jacobi sweep (smooth_jacobi, linsolve/poisson_solver.cpp:569-595):
+// out = x + omega (b - sb - A x) / D with x = in - s_in; records mean(out).
+// `which` selects the LevelScalars slot for the output mean (0: sa, 1: sx).
+// For the finest level with rz != nullptr, also accumulates (b - sb) . out.
+template <typename T, typename B>
+__global__ void __launch_bounds__(kTX* kTY)
+    k_smooth(OpInfo o, const B* __restrict__ b, const double* sb_ptr, const T* __restrict__ in,
+             const double* sin_ptr, T* __restrict__ out, LevelScalars* ls, int which, int zm,
+             SolveScalars* sc, int first_rz, int kchunk, RedBuf rb) {
+  STENCIL_PROLOGUE(o.L)
+  using A = T;
+  const double sb = *sb_ptr;
+  const A sin = A(*sin_ptr);
+  double acc[2];
+  zero(acc);
+  if(valid) {
+    for(int k = k0; k < k1; ++k) {
+      const int q = o.L.idx(i, j, k);
+      A c;
+      const A ax = apply_op<A>(o, i, j, k,
+                               [&](int ii, int jj, int kk) { return A(in[o.L.idx(ii, jj, kk)]) - sin; }, c);
+      const double bq = double(b[q]) - sb;
+      const A v = c + A(kOmega) * (A(bq) - ax) * A(inv_diag(o, i, j, k));
+      out[q] = T(v);
+      acc[0] += double(v);
+      acc[1] += bq * double(v);
+    }
+  }
+  const bool mx[2] = {false, false};
+  const int n = o.L.count();
+  reduce_finish<2>(acc, mx, rb, [=](const Sums<2>& s) {
+    const double mean = zm ? s.v[0] / n : 0.0;
+    if(which == 0) ls->sa = mean;
+    else {
+      ls->sx = mean;
+      ls->sum_x = s.v[0];
+    }
+    if(sc != nullptr) {
+      // r.z with z = out - mean (linsolve/poisson_solver.cpp:749, :791)
+      const double rz_new = s.v[1] - mean * (sc->sum_r - sc->n * sc->sr);
+      if(first_rz) {
+        sc->rz = rz_new;
+      } else {
+        sc->beta = rz_new / sc->rz;
+        sc->rz = rz_new;
+      }
+    }
+  });
+}
+
+// Residual + restriction (v_cycle :611-624 and restrict_full_weighting
+// :397-424): coarse b = mean of the children's (b - sb - A x); x = in - s_in.
+template <typename T, typename B>
+__global__ void __launch_bounds__(kTX* kTY)
+    k_restrict_residual(OpInfo o, OpInfo oc, const B* __restrict__ b, const double* sb_ptr,
+                        const T* __restrict__ in, const double* sin_ptr, T* __restrict__ bc,
+                        LevelScalars* lsc, int rx, int ry, int rz, int zm, int kchunk, RedBuf rb) {
+  STENCIL_PROLOGUE(oc.L)
+  using A = T;
+  const double sb = *sb_ptr;
+  const A sin = A(*sin_ptr);
+  const A inv_children = A(1.0 / double(rx * ry * rz));
+  double acc[1];
+  zero(acc);
+  if(valid) {
+    for(int kc = k0; kc < k1; ++kc) {
+      A sum = A(0);
+      for(int dz = 0; dz < rz; ++dz)
+        for(int dy = 0; dy < ry; ++dy)
+          for(int dx = 0; dx < rx; ++dx) {
+            const int fi = i * rx + dx, fj = j * ry + dy, fk = kc * rz + dz;
+            A c;
+            const A ax = apply_op<A>(o, fi, fj, fk,
+                                     [&](int ii, int jj, int kk) { return A(in[o.L.idx(ii, jj, kk)]) - sin; }, c);
+            sum += A(double(b[o.L.idx(fi, fj, fk)]) - sb) - ax;
+          }
+      const A v = inv_children * sum;
+      bc[oc.L.idx(i, j, kc)] = T(v);
+      acc[0] += double(v);
+    }
+  }
+  const bool mx[1] = {false};
+  const int n = oc.L.count();
+  reduce_finish<1>(acc, mx, rb, [=](const Sums<1>& s) { lsc->sb = zm ? s.v[0] / n : 0.0; });
+}
+
+// Prolongation + first post-smoothing sweep (prolongate_and_add :426-451,
+// then smooth_jacobi): x3 = (in - s_in) + (e_parent - s_e); out = x3 +
+// omega (b - sb - A x3) / D.
+template <typename T, typename B>
+__global__ void __launch_bounds__(kTX* kTY)
+    k_prolong_smooth(OpInfo o, CLay Lc, const B* __restrict__ b, const double* sb_ptr,
+                     const T* __restrict__ in, const double* sin_ptr, const T* __restrict__ ec,
+                     const double* sec_ptr, T* __restrict__ out, LevelScalars* ls, int rx, int ry,
+                     int rz, int zm, int kchunk, RedBuf rb) {
+  STENCIL_PROLOGUE(o.L)
+  using A = T;
+  const double sb = *sb_ptr;
+  const A sin = A(*sin_ptr);
+  const A sec = A(*sec_ptr);
+  double acc[1];
+  zero(acc);
+  if(valid) {
+    for(int k = k0; k < k1; ++k) {
+      const int q = o.L.idx(i, j, k);
+      A c;
+      const A ax = apply_op<A>(o, i, j, k,
+                               [&](int ii, int jj, int kk) {
+                                 return (A(in[o.L.idx(ii, jj, kk)]) - sin) +
+                                        (A(ec[Lc.idx(ii / rx, jj / ry, kk / rz)]) - sec);
+                               },
+                               c);
+      const A bq = A(double(b[q]) - sb);
+      const A v = c + A(kOmega) * (bq - ax) * A(inv_diag(o, i, j, k));
+      out[q] = T(v);
+      acc[0] += double(v);
+    }
+  }
+  const bool mx[1] = {false};
+  const int n = o.L.count();
+  reduce_finish<1>(acc, mx, rb, [=](const Sums<1>& s) { ls->sa = zm ? s.v[0] / n : 0.0; });
+}
+
+// direct_coarse_solve (linsolve/poisson_solver.cpp:530-567) with the
+// elimination precomputed on the host: row swaps, multipliers and the upper
+// factor are applied to the right-hand side in the reference's order.
+template <typename T, typename B>
+__global__ void k_coarse_solve(int n, const int* __restrict__ swaps, const double* __restrict__ f,
+                               const B* __restrict__ b, const double* sb_ptr, T* __restrict__ out,
+                               LevelScalars* ls, int zm, SolveScalars* sc, int first_rz) {
+  __shared__ double y[kMaxCoarse];
+  __shared__ double red[32];
+  const int t = threadIdx.x;
+  const double sb = *sb_ptr;
+  for(int q = t; q < n; q += blockDim.x) y[q] = double(b[q]) - sb;
+  __syncthreads();
+  if(zm && t == 0) y[n - 1] = 0.0;
+  __syncthreads();
+  for(int p = 0; p < n; ++p) {
+    if(t == 0 && swaps[p] != p) {
+      const double tmp = y[p];
+      y[p] = y[swaps[p]];
+      y[swaps[p]] = tmp;
+    }
+    __syncthreads();
+    const double yp = y[p];
+    for(int r = p + 1 + t; r < n; r += blockDim.x) {
+      const double factor = f[static_cast<size_t>(r) * n + p];
+      if(factor != 0.0) y[r] -= factor * yp;
+    }
+    __syncthreads();
+  }
+  for(int row = n - 1; row >= 0; --row) {
+    if(t == 0) y[row] = y[row] / f[static_cast<size_t>(row) * n + row];
+    __syncthreads();
+    const double yr = y[row];
+    for(int r = t; r < row; r += blockDim.x) y[r] -= f[static_cast<size_t>(r) * n + row] * yr;
+    __syncthreads();
+  }
+  // subtract_active_mean on the coarse correction
+  double part = 0.0;
+  for(int q = t; q < n; q += blockDim.x) part += y[q];
+  part = warp_sum(part);
+  if((t & 31) == 0) red[t >> 5] = part;
+  __syncthreads();
+  double mean = 0.0;
+  if(zm) {
+    double s = 0.0;
+    for(int w = 0; w < (int(blockDim.x) + 31) / 32; ++w) s += red[w];
+    mean = s / n;
+  }
+  double rzp = 0.0;
+  for(int q = t; q < n; q += blockDim.x) {
+    const double v = y[q] - mean;
+    out[q] = T(v);
+    rzp += (double(b[q]) - sb) * v;
+  }
+  __syncthreads();
+  rzp = warp_sum(rzp);
+  if((t & 31) == 0) red[t >> 5] = rzp;
+  __syncthreads();
+  if(t == 0) {
+    ls->sx = 0.0;
+    ls->sum_x = 0.0;
+    if(sc != nullptr) {
+      double s = 0.0;
+      for(int w = 0; w < (int(blockDim.x) + 31) / 32; ++w) s += red[w];
+      if(first_rz) {
+        sc->rz = s;
+      } else {
+        sc->beta = s / sc->rz;
+        sc->rz = s;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// CG kernels (FP64 vectors).
+// ---------------------------------------------------------------------------
+
+// r = (b - sb) - A (x - sx); initial residual (linsolve/poisson_solver.cpp:717-739).
+__global__ void __launch_bounds__(kTX* kTY)
+    k_initial_residual(OpInfo o, const double* __restrict__ b, const double* __restrict__ x,
+                       double* __restrict__ r, SolveScalars* sc, int kchunk, RedBuf rb) {
+  STENCIL_PROLOGUE(o.L)
+  const double sb = sc->sb, sx = sc->sx;
+  double acc[2];
+  zero(acc);
+  if(valid) {
+    for(int k = k0; k < k1; ++k) {
+      const int q = o.L.idx(i, j, k);
+      double c;
+      const double ax = apply_op<double>(o, i, j, k,
+                                         [&](int ii, int jj, int kk) { return x[o.L.idx(ii, jj, kk)] - sx; }, c);
+      const double v = (b[q] - sb) - ax;
+      r[q] = v;
+      acc[0] += v;
+      acc[1] += v * v;
+    }
+  }
+  const bool mx[2] = {false, false};
+  reduce_finish<2>(acc, mx, rb, [=](const Sums<2>& s) {
+    const int n = sc->n;
+    const double sr = sc->zero_mean ? s.v[0] / n : 0.0;
+    sc->sr = sr;
+    sc->sum_r = s.v[0];
+    const double ss = fmax(s.v[1] - n * sr * sr, 0.0);
+    const double r0 = sqrt(ss / n);
+    sc->r0 = r0;
+    sc->rnorm = r0;
+    sc->rel = r0 > 0.0 ? 1.0 : 0.0;
+    sc->iterations = 0;
+    sc->stop = 0;
+    sc->converged = r0 <= sc->tol ? 1 : 0;
+    if(sc->converged) sc->rel = 0.0;
+  });
+}
+
+// p = (z - sz) + beta (p - sp); first iteration p = z - sz.
+template <typename T>
+__global__ void __launch_bounds__(kTX* kTY)
+    k_update_p(CLay L, const T* __restrict__ z, const LevelScalars* ls0, double* __restrict__ p,
+               SolveScalars* sc, int first, int kchunk, RedBuf rb) {
+  STENCIL_PROLOGUE(L)
+  const double sz = ls0->sx;
+  const double beta = first ? 0.0 : sc->beta;
+  const double sp = sc->sp;
+  double acc[1];
+  zero(acc);
+  if(valid) {
+    for(int k = k0; k < k1; ++k) {
+      const int q = L.idx(i, j, k);
+      const double v = first ? double(z[q]) - sz : (double(z[q]) - sz) + beta * (p[q] - sp);
+      p[q] = v;
+      acc[0] += v;
+    }
+  }
+  const bool mx[1] = {false};
+  reduce_finish<1>(acc, mx, rb, [=](const Sums<1>& s) {
+    sc->sp = sc->zero_mean ? s.v[0] / sc->n : 0.0;
+  });
+}
+
+// Ap = A (p - sp); mean shift of Ap; p.Ap; alpha (linsolve/poisson_solver.cpp:751-761).
+__global__ void __launch_bounds__(kTX* kTY)
+    k_apply_ap(OpInfo o, const double* __restrict__ p, double* __restrict__ ap, SolveScalars* sc,
+               int kchunk, RedBuf rb) {
+  STENCIL_PROLOGUE(o.L)
+  const double sp = sc->sp;
+  double acc[3];
+  zero(acc);
+  if(valid) {
+    for(int k = k0; k < k1; ++k) {
+      const int q = o.L.idx(i, j, k);
+      double c;
+      const double v = apply_op<double>(o, i, j, k,
+                                        [&](int ii, int jj, int kk) { return p[o.L.idx(ii, jj, kk)] - sp; }, c);
+      ap[q] = v;
+      acc[0] += v;
+      acc[1] += c * v;
+      acc[2] += c;
+    }
+  }
+  const bool mx[3] = {false, false, false};
+  reduce_finish<3>(acc, mx, rb, [=](const Sums<3>& s) {
+    const double sap = sc->zero_mean ? s.v[0] / sc->n : 0.0;
+    sc->sap = sap;
+    const double pap = s.v[1] - sap * s.v[2];
+    sc->pap = pap;
+    if(fabs(pap) < kSmallNumber) {
+      sc->stop = 1;
+    } else {
+      sc->alpha = sc->rz / pap;
+    }
+  });
+}
+
+// x = (x - sx) + alpha (p - sp); r = (r - sr) - alpha (Ap - sap); norms and
+// the convergence test (linsolve/poisson_solver.cpp:762-782).
+__global__ void __launch_bounds__(kTX* kTY)
+    k_update_xr(CLay L, double* __restrict__ x, double* __restrict__ r,
+                const double* __restrict__ p, const double* __restrict__ ap, SolveScalars* sc,
+                int kchunk, RedBuf rb) {
+  STENCIL_PROLOGUE(L)
+  const int stop = sc->stop;
+  const double alpha = sc->alpha, sx = sc->sx, sr = sc->sr, sp = sc->sp, sap = sc->sap;
+  double acc[3];
+  zero(acc);
+  if(valid && !stop) {
+    for(int k = k0; k < k1; ++k) {
+      const int q = L.idx(i, j, k);
+      const double xv = (x[q] - sx) + alpha * (p[q] - sp);
+      const double rv = (r[q] - sr) - alpha * (ap[q] - sap);
+      x[q] = xv;
+      r[q] = rv;
+      acc[0] += xv;
+      acc[1] += rv;
+      acc[2] += rv * rv;
+    }
+  }
+  const bool mx[3] = {false, false, false};
+  reduce_finish<3>(acc, mx, rb, [=](const Sums<3>& s) {
+    if(sc->stop) return;
+    const int n = sc->n;
+    const int zm = sc->zero_mean;
+    sc->sx = zm ? s.v[0] / n : 0.0;
+    const double srn = zm ? s.v[1] / n : 0.0;
+    sc->sr = srn;
+    sc->sum_r = s.v[1];
+    const double ss = fmax(s.v[2] - n * srn * srn, 0.0);
+    sc->rnorm = sqrt(ss / n);
+    sc->iterations += 1;
+    sc->rel = sc->r0 > 0.0 ? sc->rnorm / sc->r0 : 0.0;
+    if(sc->rel <= sc->tol) sc->converged = 1;
+  });
+}
+
+__global__ void k_compact_to_pressure(Grid g, const double* __restrict__ x, const SolveScalars* sc,
+                                      double* __restrict__ p) {
+  const Lay P = make_lay(g, kCell);
+  const CLay L = make_clay(g.nx, g.ny, g.nz);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z;
+  if(i >= L.nx || j >= L.ny) return;
+  p[P.idx(i + 1, j + 1, k + 1)] = x[L.idx(i, j, k)] - sc->sx;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Plan
+// ---------------------------------------------------------------------------
+
+struct Level {
+  Grid g;
+  CLay L;
+  OpInfo op;
+  void* a = nullptr;   // smoother output a
+  void* x = nullptr;   // smoother output b (correction)
+  void* b = nullptr;   // rhs (levels >= 1)
+  double* invd = nullptr;
+  int rx = 1, ry = 1, rz = 1;  // refinement ratio to the next coarser level
+};
+
+struct PoissonPlan {
+  Grid g;
+  PBC pbc;
+  int precision = 0;
+  int zero_mean = 1;
+  std::vector<Level> levels;
+  int coarse_n = 0;
+  int* swaps = nullptr;
+  double* factors = nullptr;
+  LevelScalars* ls = nullptr;  // device, one per level
+  double *b = nullptr, *x = nullptr, *r = nullptr, *p = nullptr, *ap = nullptr;
+  size_t bytes = 0;
+};
+
+namespace {
+
+bool can_coarsen_axis(int cells) { return cells > 1 && cells % 2 == 0 && cells > 2; }
+
+OpInfo make_op(const Grid& g, const PBC& pbc) {
+  OpInfo o;
+  o.L = make_clay(g.nx, g.ny, g.nz);
+  for(int a = 0; a < 3; ++a) {
+    const double h = g.h(a);
+    o.inv2[a] = 1.0 / (h * h);
+    o.periodic[a] = pbc.type[2 * a] == kPPeriodic ? 1 : 0;
+    o.dir_lo[a] = pbc.type[2 * a] == kPDirichlet ? 1 : 0;
+    o.dir_hi[a] = pbc.type[2 * a + 1] == kPDirichlet ? 1 : 0;
+  }
+  o.invd = nullptr;
+  return o;
+}
+
+// compute_operator_diagonal (linsolve/poisson_solver.cpp:271-314) by boundary class.
+std::vector<double> inverse_diagonal_table(const Grid& g, const PBC& pbc) {
+  std::vector<double> t(64, 0.0);
+  for(int cz = 0; cz < 4; ++cz)
+    for(int cy = 0; cy < 4; ++cy)
+      for(int cx = 0; cx < 4; ++cx) {
+        const int cls[3] = {cx, cy, cz};
+        double value = 0.0;
+        for(int a = 0; a < 3; ++a) {
+          const double inv = 1.0 / std::pow(g.h(a), 2.0);
+          double coefficient = 2.0 * inv;
+          if(pbc.type[2 * a] == kPPeriodic) {
+            value += coefficient;
+            continue;
+          }
+          const bool first = cls[a] == 1 || cls[a] == 3;
+          const bool last = cls[a] == 2 || cls[a] == 3;
+          if(first) coefficient += pbc.type[2 * a] == kPDirichlet ? inv : -inv;
+          if(last) coefficient += pbc.type[2 * a + 1] == kPDirichlet ? inv : -inv;
+          value += coefficient;
+        }
+        t[cx + 4 * cy + 16 * cz] = value != 0.0 ? 1.0 / value : 0.0;
+      }
+  return t;
+}
+
+// Host copy of apply_poisson_operator with homogeneous rules, for assembling
+// the coarse matrix column by column as direct_coarse_solve does.
+void host_apply(const Grid& g, const PBC& pbc, const std::vector<double>& in,
+                std::vector<double>& out) {
+  const CLay L = make_clay(g.nx, g.ny, g.nz);
+  auto val = [&](int i, int j, int k) { return in[L.idx(i, j, k)]; };
+  for(int k = 0; k < L.nz; ++k)
+    for(int j = 0; j < L.ny; ++j)
+      for(int i = 0; i < L.nx; ++i) {
+        const double c = val(i, j, k);
+        const int pos[3] = {i, j, k};
+        double nb[3][2];
+        for(int a = 0; a < 3; ++a) {
+          for(int s = 0; s < 2; ++s) {
+            int q[3] = {i, j, k};
+            const bool upper = s == 1;
+            const int n = L.n(a);
+            if((!upper && pos[a] > 0) || (upper && pos[a] < n - 1)) {
+              q[a] += upper ? 1 : -1;
+              nb[a][s] = val(q[0], q[1], q[2]);
+              continue;
+            }
+            const int type = pbc.type[2 * a + s];
+            if(type == kPPeriodic) {
+              q[a] = upper ? 0 : n - 1;
+              nb[a][s] = val(q[0], q[1], q[2]);
+            } else if(type == kPNeumann) {
+              nb[a][s] = c;
+            } else {
+              nb[a][s] = -c;
+            }
+          }
+        }
+        out[L.idx(i, j, k)] = -(nb[0][1] - 2.0 * c + nb[0][0]) / (g.dx * g.dx) -
+                              (nb[1][1] - 2.0 * c + nb[1][0]) / (g.dy * g.dy) -
+                              (nb[2][1] - 2.0 * c + nb[2][0]) / (g.dz * g.dz);
+      }
+}
+
+}  // namespace
+
+PoissonPlan* poisson_plan_create(const Grid& g, const PBC& pbc_in, int precision) {
+  auto* P = new PoissonPlan();
+  P->g = g;
+  // homogeneous_boundary_conditions (linsolve/poisson_solver.cpp:164-173)
+  P->pbc = pbc_in;
+  for(int f = 0; f < 6; ++f) {
+    P->pbc.value[f] = 0.0;
+    P->pbc.gradient[f] = 0.0;
+  }
+  P->precision = precision;
+  P->zero_mean = 1;
+  for(int f = 0; f < 6; ++f)
+    if(pbc_in.type[f] == kPDirichlet) P->zero_mean = 0;
+  const size_t tsz = precision == 1 ? sizeof(float) : sizeof(double);
+
+  // build_hierarchy (linsolve/poisson_solver.cpp:316-384)
+  Grid cur = g;
+  for(;;) {
+    Level lv;
+    lv.g = cur;
+    lv.L = make_clay(cur.nx, cur.ny, cur.nz);
+    lv.op = make_op(cur, P->pbc);
+    P->levels.push_back(lv);
+    if(!(can_coarsen_axis(cur.nx) || can_coarsen_axis(cur.ny) || can_coarsen_axis(cur.nz))) break;
+    Grid c = cur;
+    if(can_coarsen_axis(cur.nx)) { c.nx = cur.nx / 2; c.dx = 2.0 * cur.dx; }
+    if(can_coarsen_axis(cur.ny)) { c.ny = cur.ny / 2; c.dy = 2.0 * cur.dy; }
+    if(can_coarsen_axis(cur.nz)) { c.nz = cur.nz / 2; c.dz = 2.0 * cur.dz; }
+    if(c.nx == cur.nx && c.ny == cur.ny && c.nz == cur.nz) break;
+    Level& prev = P->levels.back();
+    prev.rx = cur.nx == c.nx ? 1 : 2;
+    prev.ry = cur.ny == c.ny ? 1 : 2;
+    prev.rz = cur.nz == c.nz ? 1 : 2;
+    cur = c;
+  }
+  const int nl = static_cast<int>(P->levels.size());
+  for(int l = 0; l < nl; ++l) {
+    Level& lv = P->levels[l];
+    const size_t n = lv.L.count();
+    OFB_CHECK(cudaMalloc(&lv.a, n * tsz));
+    OFB_CHECK(cudaMalloc(&lv.x, n * tsz));
+    P->bytes += 2 * n * tsz;
+    if(l > 0) {
+      OFB_CHECK(cudaMalloc(&lv.b, n * tsz));
+      P->bytes += n * tsz;
+    }
+    std::vector<double> t = inverse_diagonal_table(lv.g, P->pbc);
+    OFB_CHECK(cudaMalloc(&lv.invd, 64 * sizeof(double)));
+    OFB_CHECK(cudaMemcpy(lv.invd, t.data(), 64 * sizeof(double), cudaMemcpyHostToDevice));
+    lv.op.invd = lv.invd;
+  }
+  OFB_CHECK(cudaMalloc(&P->ls, nl * sizeof(LevelScalars)));
+  OFB_CHECK(cudaMemset(P->ls, 0, nl * sizeof(LevelScalars)));
+
+  // coarsest-grid elimination (direct_coarse_solve / gaussian_elimination,
+  // linsolve/poisson_solver.cpp:482-567), done once on the host
+  const Level& co = P->levels.back();
+  const int n = co.L.count();
+  if(n > kMaxCoarse) {
+    poisson_plan_destroy(P);
+    throw std::invalid_argument("coarsest multigrid level has " + std::to_string(n) +
+                                " unknowns; at most " + std::to_string(kMaxCoarse) +
+                                " are supported");
+  }
+  P->coarse_n = n;
+  std::vector<double> m(static_cast<size_t>(n) * n, 0.0), e(n, 0.0), img(n, 0.0);
+  for(int col = 0; col < n; ++col) {
+    std::fill(e.begin(), e.end(), 0.0);
+    e[col] = 1.0;
+    host_apply(co.g, P->pbc, e, img);
+    for(int row = 0; row < n; ++row) m[static_cast<size_t>(row) * n + col] = img[row];
+  }
+  if(P->zero_mean)
+    for(int col = 0; col < n; ++col) m[static_cast<size_t>(n - 1) * n + col] = 1.0;
+  std::vector<int> swaps(n);
+  for(int piv = 0; piv < n; ++piv) {
+    int best = piv;
+    double best_abs = std::fabs(m[static_cast<size_t>(piv) * n + piv]);
+    for(int row = piv + 1; row < n; ++row) {
+      const double cand = std::fabs(m[static_cast<size_t>(row) * n + piv]);
+      if(cand > best_abs) {
+        best = row;
+        best_abs = cand;
+      }
+    }
+    if(best_abs < kSmallNumber) {
+      poisson_plan_destroy(P);
+      throw std::runtime_error("direct coarse solve encountered a singular matrix");
+    }
+    swaps[piv] = best;
+    // Columns left of the pivot hold the multipliers of earlier steps; they
+    // stay with their row position so the device replays the eliminations
+    // on the right-hand side in the reference's order.
+    if(best != piv)
+      for(int c = piv; c < n; ++c)
+        std::swap(m[static_cast<size_t>(piv) * n + c], m[static_cast<size_t>(best) * n + c]);
+    const double inv = 1.0 / m[static_cast<size_t>(piv) * n + piv];
+    for(int row = piv + 1; row < n; ++row) {
+      const double factor = m[static_cast<size_t>(row) * n + piv] * inv;
+      if(std::fabs(factor) < kSmallNumber) {
+        m[static_cast<size_t>(row) * n + piv] = 0.0;
+        continue;
+      }
+      for(int c = piv + 1; c < n; ++c)
+        m[static_cast<size_t>(row) * n + c] -= factor * m[static_cast<size_t>(piv) * n + c];
+      m[static_cast<size_t>(row) * n + piv] = factor;  // keep the multiplier
+    }
+  }
+  OFB_CHECK(cudaMalloc(&P->swaps, n * sizeof(int)));
+  OFB_CHECK(cudaMalloc(&P->factors, static_cast<size_t>(n) * n * sizeof(double)));
+  OFB_CHECK(cudaMemcpy(P->swaps, swaps.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+  OFB_CHECK(cudaMemcpy(P->factors, m.data(), static_cast<size_t>(n) * n * sizeof(double),
+                       cudaMemcpyHostToDevice));
+
+  const size_t nf = P->levels[0].L.count();
+  OFB_CHECK(cudaMalloc(&P->b, nf * sizeof(double)));
+  OFB_CHECK(cudaMalloc(&P->x, nf * sizeof(double)));
+  OFB_CHECK(cudaMalloc(&P->r, nf * sizeof(double)));
+  OFB_CHECK(cudaMalloc(&P->p, nf * sizeof(double)));
+  OFB_CHECK(cudaMalloc(&P->ap, nf * sizeof(double)));
+  OFB_CHECK(cudaMemset(P->p, 0, nf * sizeof(double)));
+  P->bytes += 5 * nf * sizeof(double);
+  return P;
+}
+
+void poisson_plan_destroy(PoissonPlan* P) {
+  if(P == nullptr) return;
+  for(Level& lv : P->levels) {
+    cudaFree(lv.a);
+    cudaFree(lv.x);
+    cudaFree(lv.b);
+    cudaFree(lv.invd);
+  }
+  cudaFree(P->ls);
+  cudaFree(P->swaps);
+  cudaFree(P->factors);
+  cudaFree(P->b);
+  cudaFree(P->x);
+  cudaFree(P->r);
+  cudaFree(P->p);
+  cudaFree(P->ap);
+  delete P;
+}
+
+int poisson_levels(const PoissonPlan* P) { return static_cast<int>(P->levels.size()); }
+int poisson_coarse_unknowns(const PoissonPlan* P) { return P->coarse_n; }
+size_t poisson_device_bytes(const PoissonPlan* P) { return P->bytes; }
+double* poisson_b(PoissonPlan* P) { return P->b; }
+double* poisson_x(PoissonPlan* P) { return P->x; }
+
+namespace {
+
+// v_cycle (linsolve/poisson_solver.cpp:597-633) from level l; the finest
+// level's rhs is the CG residual (double, shift sc->sr).
+template <typename T>
+void v_cycle(PoissonPlan* P, int l, SolveScalars* sc, int first_rz, RedBuf rb, cudaStream_t s) {
+  Level& lv = P->levels[l];
+  const int nl = static_cast<int>(P->levels.size());
+  const int zm = P->zero_mean;
+  LevelScalars* ls = P->ls + l;
+  const double* sb_ptr = l == 0 ? &sc->sr : &ls->sb;
+  SolveScalars* rz_sc = l == 0 ? sc : nullptr;
+  T* a = static_cast<T*>(lv.a);
+  T* x = static_cast<T*>(lv.x);
+  if(l + 1 == nl) {
+    if(l == 0)
+      k_coarse_solve<T, double><<<1, 256, 0, s>>>(P->coarse_n, P->swaps, P->factors, P->r, sb_ptr,
+                                                  x, ls, zm, rz_sc, first_rz);
+    else
+      k_coarse_solve<T, T><<<1, 256, 0, s>>>(P->coarse_n, P->swaps, P->factors,
+                                            static_cast<const T*>(lv.b), sb_ptr, x, ls, zm,
+                                            rz_sc, first_rz);
+    OFB_LAUNCH_CHECK("k_coarse_solve");
+    return;
+  }
+  const Launch3 ln = launch3(lv.L.nx, lv.L.ny, lv.L.nz);
+  Level& cv = P->levels[l + 1];
+  const Launch3 lc = launch3(cv.L.nx, cv.L.ny, cv.L.nz);
+  LevelScalars* lsc = P->ls + (l + 1);
+  auto smooth_chain = [&](auto* bptr) {
+    using B = std::remove_cv_t<std::remove_pointer_t<decltype(bptr)>>;
+    k_smooth_first<T, B><<<ln.grid, ln.block, 0, s>>>(lv.op, bptr, sb_ptr, a, ls, zm, ln.kchunk, rb);
+    k_smooth<T, B><<<ln.grid, ln.block, 0, s>>>(lv.op, bptr, sb_ptr, a, &ls->sa, x, ls, 1, zm,
+                                                nullptr, 0, ln.kchunk, rb);
+    k_restrict_residual<T, B><<<lc.grid, lc.block, 0, s>>>(lv.op, cv.op, bptr, sb_ptr, x, &ls->sx,
+                                                           static_cast<T*>(cv.b), lsc, lv.rx,
+                                                           lv.ry, lv.rz, zm, lc.kchunk, rb);
+    OFB_LAUNCH_CHECK("v_cycle descent");
+    v_cycle<T>(P, l + 1, sc, first_rz, rb, s);
+    k_prolong_smooth<T, B><<<ln.grid, ln.block, 0, s>>>(lv.op, cv.L, bptr, sb_ptr, x, &ls->sx,
+                                                        static_cast<const T*>(cv.x), &lsc->sx, a,
+                                                        ls, lv.rx, lv.ry, lv.rz, zm, ln.kchunk, rb);
+    k_smooth<T, B><<<ln.grid, ln.block, 0, s>>>(lv.op, bptr, sb_ptr, a, &ls->sa, x, ls, 1, zm,
+                                                rz_sc, first_rz, ln.kchunk, rb);
+    OFB_LAUNCH_CHECK("v_cycle ascent");
+  };
+  if(l == 0) smooth_chain(static_cast<const double*>(P->r));
+  else smooth_chain(static_cast<const T*>(lv.b));
+}
+
+template <typename T>
+void solve_impl(PoissonPlan* P, int max_iterations, double tolerance, SolveScalars* sc,
+                SolveScalars* host, RedBuf rb, cudaStream_t s, double* history, int history_cap) {
+  const Level& l0 = P->levels[0];
+  const Launch3 ln = launch3(l0.L.nx, l0.L.ny, l0.L.nz);
+  // sc->sb and sc->sx were set by the kernels that filled b and x.
+  SolveScalars init{};
+  OFB_CHECK(cudaMemcpyAsync(host, sc, sizeof(SolveScalars), cudaMemcpyDeviceToHost, s));
+  OFB_CHECK(cudaStreamSynchronize(s));
+  init = *host;
+  init.zero_mean = P->zero_mean;
+  init.n = l0.L.count();
+  init.tol = tolerance;
+  if(!P->zero_mean) {
+    init.sb = 0.0;
+    init.sx = 0.0;
+    init.removed_rhs_mean = 0.0;
+  }
+  init.sp = 0.0;
+  OFB_CHECK(cudaMemcpyAsync(sc, &init, sizeof(SolveScalars), cudaMemcpyHostToDevice, s));
+  k_initial_residual<<<ln.grid, ln.block, 0, s>>>(l0.op, P->b, P->x, P->r, sc, ln.kchunk, rb);
+  OFB_LAUNCH_CHECK("k_initial_residual");
+  OFB_CHECK(cudaMemcpyAsync(host, sc, sizeof(SolveScalars), cudaMemcpyDeviceToHost, s));
+  OFB_CHECK(cudaStreamSynchronize(s));
+  int nh = 0;
+  if(history && nh < history_cap) history[nh] = host->r0;
+  ++nh;
+  if(host->converged) return;
+  v_cycle<T>(P, 0, sc, 1, rb, s);
+  k_update_p<T><<<ln.grid, ln.block, 0, s>>>(l0.L, static_cast<const T*>(l0.x), P->ls, P->p, sc, 1,
+                                             ln.kchunk, rb);
+  OFB_LAUNCH_CHECK("k_update_p");
+  for(int it = 0; it < max_iterations; ++it) {
+    k_apply_ap<<<ln.grid, ln.block, 0, s>>>(l0.op, P->p, P->ap, sc, ln.kchunk, rb);
+    k_update_xr<<<ln.grid, ln.block, 0, s>>>(l0.L, P->x, P->r, P->p, P->ap, sc, ln.kchunk, rb);
+    OFB_LAUNCH_CHECK("k_update_xr");
+    OFB_CHECK(cudaMemcpyAsync(host, sc, sizeof(SolveScalars), cudaMemcpyDeviceToHost, s));
+    OFB_CHECK(cudaStreamSynchronize(s));
+    if(host->stop) break;
+    if(history && nh < history_cap) history[nh] = host->rnorm;
+    ++nh;
+    if(host->converged) break;
+    v_cycle<T>(P, 0, sc, 0, rb, s);
+    k_update_p<T><<<ln.grid, ln.block, 0, s>>>(l0.L, static_cast<const T*>(l0.x), P->ls, P->p, sc,
+                                               0, ln.kchunk, rb);
+    OFB_LAUNCH_CHECK("k_update_p");
+  }
+}
+
+}  // namespace
+
+void poisson_solve(PoissonPlan* P, int max_iterations, double tolerance, SolveScalars* sc_dev,
+                   SolveScalars* sc_host, RedBuf rb, cudaStream_t s, double* history,
+                   int history_cap) {
+  if(P->precision == 1)
+    solve_impl<float>(P, max_iterations, tolerance, sc_dev, sc_host, rb, s, history, history_cap);
+  else
+    solve_impl<double>(P, max_iterations, tolerance, sc_dev, sc_host, rb, s, history, history_cap);
+  OFB_CHECK(cudaMemcpyAsync(sc_host, sc_dev, sizeof(SolveScalars), cudaMemcpyDeviceToHost, s));
+  OFB_CHECK(cudaStreamSynchronize(s));
+}
+
+void launch_compact_to_pressure(const Grid& g, const double* x, const SolveScalars* sc,
+                                double* p_padded, cudaStream_t s) {
+  dim3 block(32, 8, 1);
+  dim3 grid((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz);
+  k_compact_to_pressure<<<grid, block, 0, s>>>(g, x, sc, p_padded);
+  OFB_LAUNCH_CHECK("k_compact_to_pressure");
+}
+
+}  // namespace ofb

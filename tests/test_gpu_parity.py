@@ -1,0 +1,157 @@
+"""GPU parity against the CPU oracle, through the C ABI (include/orchard_b200.h).
+
+Tolerances: the FP64 path must match the reference's deterministic CPU build
+to a max-norm relative difference of 1e-11 (velocity and pressure after N
+steps); single operators are compared at 1e-12.  Sums on the GPU use a
+different (tree) order than the CPU's sequential loops, so results differ at
+the rounding level, never more.
+"""
+import numpy as np
+import pytest
+
+import pyoracle as po
+from conftest import rel_maxdiff, to_gpu_bc, to_gpu_grid, to_gpu_pbc
+
+pytestmark = pytest.mark.gpu
+
+STEP_TOL = 1e-11
+OP_TOL = 1e-12
+
+
+@pytest.fixture(scope="module")
+def sb():
+    import solver_b200
+    return solver_b200
+
+
+def _random_velocity(grid, rng, amp=1.0):
+    return [rng.standard_normal(po.shape(grid, c)) * amp for c in "uvw"]
+
+
+def _tg_gpu_run(sb, oracle, cfg, steps, mode=0, variant=0):
+    g = oracle.tg_grid(cfg)
+    bc = oracle.tg_bc(cfg)
+    dt = oracle.tg_dt(cfg)
+    s0 = oracle.tg_init(cfg, 0)
+    ctx = sb.Context(to_gpu_grid(g), to_gpu_bc(bc))
+    ctx.upload_state(s0.u, s0.v, s0.w, s0.adv_u, s0.adv_v, s0.adv_w, s0.p, s0.has_previous_advection,
+                     s0.metrics)
+    prm = sb.step_params(cfg.viscosity, dt, cfg.poisson_max_iterations, cfg.poisson_tolerance)
+    metrics = ctx.run_steps(prm, steps)
+    out = ctx.download_state()
+    ref = oracle.tg_steps(cfg, steps, s0.copy())
+    return out, ref, metrics
+
+
+@pytest.mark.parametrize("n,steps", [((32, 32, 1), 5), ((16, 16, 16), 3), ((12, 10, 8), 3)])
+def test_taylor_green_steps_match_oracle(sb, oracle, n, steps):
+    cfg = po.steps_config(*n, 0.01, 0.5, steps, 1e-12)
+    out, ref, metrics = _tg_gpu_run(sb, oracle, cfg, steps)
+    for name in ("u", "v", "w", "p", "adv_u", "adv_v", "adv_w"):
+        d = rel_maxdiff(out[name], getattr(ref, name))
+        assert d <= STEP_TOL, (name, d)
+    assert metrics["step"] == ref.metrics["step"] == steps
+    assert metrics["pressure_iterations"] == ref.metrics["pressure_iterations"]
+    assert abs(metrics["max_cfl"] - ref.metrics["max_cfl"]) <= 1e-12 * ref.metrics["max_cfl"]
+    assert metrics["divergence_l2"] <= 1e-10
+
+
+def test_cavity_steps_match_oracle(sb, oracle):
+    cc = po.cavity_config(32, 32, poisson_tolerance=1e-12)
+    g = oracle.cavity_grid(cc)
+    bc = oracle.cavity_bc(cc)
+    s0 = oracle.cavity_init(cc)
+    ctx = sb.Context(to_gpu_grid(g), to_gpu_bc(bc))
+    ctx.upload_state(s0.u, s0.v, s0.w, s0.adv_u, s0.adv_v, s0.adv_w, s0.p, 0, s0.metrics)
+    nu = cc.lid_velocity / cc.reynolds
+    prm = sb.step_params(nu, oracle.cavity_dt(cc), cc.poisson_max_iterations, cc.poisson_tolerance,
+                         variant=sb.OF_CORRECTION_CAVITY)
+    m = ctx.run_steps(prm, 6)
+    out = ctx.download_state()
+    ref = oracle.cavity_steps(cc, 6, s0.copy())
+    for name in ("u", "v", "p"):
+        d = rel_maxdiff(out[name], getattr(ref, name))
+        assert d <= STEP_TOL, (name, d)
+    assert m["pressure_iterations"] == ref.metrics["pressure_iterations"]
+
+
+def test_advection_matches_oracle(sb, oracle):
+    rng = np.random.default_rng(1)
+    g = po.Grid(12, 9, 7, 0.3, 0.25, 0.4)
+    u, v, w = _random_velocity(g, rng)
+    ctx = sb.Context(to_gpu_grid(g), [sb.PERIODIC] * 6)
+    got = ctx.compute_advection_term(u, v, w)
+    exp = oracle.advection(g, u, v, w)
+    for a, b in zip(got, exp):
+        assert rel_maxdiff(a, b) <= OP_TOL
+
+
+@pytest.mark.parametrize("types", [
+    [po.PERIODIC] * 6,
+    [po.NO_SLIP_WALL, po.NO_SLIP_WALL, po.NO_SLIP_WALL, po.PRESCRIBED_VELOCITY, po.SYMMETRY,
+     po.SYMMETRY],
+    [po.PERIODIC, po.PERIODIC, po.NO_SLIP_WALL, po.PRESCRIBED_VELOCITY, po.PERIODIC, po.PERIODIC],
+])
+def test_predictor_adi_matches_oracle(sb, oracle, types):
+    rng = np.random.default_rng(2)
+    g = po.Grid(10, 8, 6, 0.2, 0.3, 0.25)
+    vel = [None] * 6
+    vel[3] = (0.7, 0.0, 0.1)
+    bc = po.bc_from(types, vel)
+    rhs = _random_velocity(g, rng)
+    ctx = sb.Context(to_gpu_grid(g), to_gpu_bc(bc))
+    got, lines = ctx.solve_predictor_adi(rhs, 0.05)
+    exp, lines_ref = oracle.predictor_adi(g, bc, 0.05, *rhs)
+    assert lines == lines_ref
+    for a, b in zip(got, exp):
+        assert rel_maxdiff(a, b) <= OP_TOL
+
+
+@pytest.mark.parametrize("case", ["dirichlet2d", "neumann2d", "periodic3d", "mixed3d"])
+def test_poisson_matches_oracle(sb, oracle, case):
+    rng = np.random.default_rng(3)
+    if case == "dirichlet2d":
+        g = po.Grid(32, 32, 1, 1 / 32, 1 / 32, 1.0)
+        types = [po.P_DIRICHLET] * 4 + [po.P_NEUMANN] * 2
+        vals = [0.3, -0.1, 0.2, 0.0, 0.0, 0.0]
+        pbc = po.pbc_from(types, vals)
+    elif case == "neumann2d":
+        g = po.Grid(24, 24, 1, 1 / 24, 1 / 24, 1.0)
+        pbc = po.pbc_from([po.P_NEUMANN] * 6, gradients=[0.1, 0.1, -0.2, -0.2, 0.0, 0.0])
+    elif case == "periodic3d":
+        g = po.Grid(16, 16, 16, 0.39, 0.39, 0.39)
+        pbc = po.pbc_from([po.P_PERIODIC] * 6)
+    else:
+        g = po.Grid(16, 8, 12, 0.1, 0.2, 0.15)
+        pbc = po.pbc_from([po.P_PERIODIC, po.P_PERIODIC, po.P_NEUMANN, po.P_DIRICHLET,
+                           po.P_NEUMANN, po.P_NEUMANN])
+    rhs = rng.standard_normal(po.shape(g, "p"))
+    ctx = sb.Context(to_gpu_grid(g), [sb.PERIODIC] * 6)
+    p_gpu, d = ctx.solve_pressure_poisson(rhs, to_gpu_pbc(pbc), 200, 1e-12)
+    p_ref = np.zeros(po.shape(g, "p"))
+    dref, hist = oracle.poisson_solve(g, pbc, 200, 1e-12, rhs, p_ref)
+    assert d["converged"] and dref.converged
+    assert d["iterations"] == dref.iterations
+    assert d["multigrid_levels"] == dref.multigrid_levels
+    assert d["coarse_unknowns"] == dref.coarse_unknowns
+    assert d["zero_mean_enforced"] == bool(dref.zero_mean_enforced)
+    assert rel_maxdiff(p_gpu, p_ref) <= 1e-11
+    # near convergence the norms are rounding-dominated: compare against r0
+    np.testing.assert_allclose(d["residual_history"], hist, rtol=1e-9, atol=1e-10 * hist[0])
+
+
+def test_project_velocity_matches_oracle(sb, oracle):
+    rng = np.random.default_rng(4)
+    g = po.Grid(16, 12, 10, 0.2, 0.25, 0.3)
+    bc = po.periodic_bc()
+    pred = _random_velocity(g, rng)
+    ctx = sb.Context(to_gpu_grid(g), to_gpu_bc(bc))
+    (cu, cv, cw), phi, rhs, d = ctx.project_velocity(pred, 0.01, 1.0, 200, 1e-12)
+    exp, rhs_ref, dref = oracle.project_velocity(g, bc, 0.01, 1.0, 200, 1e-12, *pred,
+                                                 np.zeros(po.shape(g, "p")))
+    for a, b in zip((cu, cv, cw), exp):
+        assert rel_maxdiff(a, b) <= OP_TOL * 10
+    assert rel_maxdiff(rhs, rhs_ref) <= OP_TOL
+    assert d["pressure_solve"]["iterations"] == dref.pressure_solve.iterations
+    assert d["divergence_l2_after"] <= 1e-10
+    assert abs(d["divergence_l2_before"] - dref.divergence_l2_before) <= 1e-12 * dref.divergence_l2_before
