@@ -1,0 +1,411 @@
+#!/usr/bin/env python
+"""Benchmark: 3D Taylor-Green 256^3 projection steps per second on B200.
+
+Workload (the reference's headline path): 3D periodic Taylor-Green on
+[0, 2 pi]^3 at 256^3, nu = 1/1600, CFL 0.5 (fixed dt = 0.5 / sum(1/h)),
+u = sin x cos y cos z, v = -cos x sin y cos z, w = 0, MG-PCG pressure solve to
+relative residual 1e-12, FP64 (``--precision mixed``: FP32 V-cycle inside the
+FP64 CG).  One bench "step" is one full projection time step (TVD advection,
+ADI Helmholtz predictor, MG-PCG Poisson, divergence/gradient correction) on
+the resident state.  Every field of the 256^3 state (138 MB) is larger than
+the 126 MB L2, so no L2 flush is needed between steps.
+
+Arms:
+  --impl b200 (default)   this repository's CUDA path through its C ABI;
+  --impl reference        the reference's own CPU implementation of the same
+                          step (oracle/_ref, the reference's sources compiled
+                          in place; the plain-C oracle port if that build is
+                          absent), one process per host core.
+
+Multi-GPU: the path does not shard (replicas only): each rank runs its own
+independent 256^3 simulation; value = total steps/s over ranks, time = max
+over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_DEFAULT = 256
+NU = 1.0 / 1600.0
+CFL = 0.5
+TOL = 1e-12
+MAX_IT = 400
+METRIC = "TGV 256^3 steps/s (FP64 projection step)"
+
+
+def tg_dt(n, cfl=CFL):
+    h = 2.0 * math.pi / n
+    return cfl / (3.0 / h)
+
+
+# ---------------------------------------------------------------------------
+# algorithmic bytes per launch of each kernel class (compulsory traffic: each
+# distinct input read once, each output written once), N = active cells
+# ---------------------------------------------------------------------------
+
+def bytes_per_launch(n, precision):
+    N = n ** 3
+    d = 8
+    t = 4 if precision == "mixed" else 8  # V-cycle level vectors
+    return {
+        "predictor_rhs": 13 * d * N / 3,  # per component launch (7 reads, 6 writes over 3)
+        "adi_sweep": 2 * d * N,
+        "divergence_rhs": 5 * d * N,
+        "pcg_initial_residual": 3 * d * N,
+        "pcg_apply_ap": 2 * d * N,
+        "pcg_update_xr": 6 * d * N,
+        "pcg_update_p": (2 * d + t) * N,
+        "vcycle_smooth_first_fine": (d + t) * N,
+        "vcycle_smooth_fine": (d + 2 * t) * N,
+        "vcycle_restrict_fine": (d + t + t / 8) * N,
+        "vcycle_prolong_smooth_fine": (d + 2 * t + t / 8) * N,
+        "correct_velocity": (1 + 3 + 3) * d * N / 3 + d * N,  # per component launch
+        "cell_pass": 7 * d * N,
+    }
+
+
+def read_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def read_traffic():
+    """Per-launch DRAM bytes from the committed ncu summary (profiles/)."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    out = {}
+    if os.path.exists(p):
+        with open(p) as f:
+            for line in f:
+                line = line.strip()
+                if not line or line.startswith("#"):
+                    continue
+                parts = line.split()
+                if len(parts) >= 2:
+                    try:
+                        out[parts[0]] = float(parts[1])
+                    except ValueError:
+                        pass
+    return out
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(prefix="clocks_", suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        if self.proc is None:
+            return out
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for name, val in zip(names, parts[5:9]):
+                    if val.lower() == "active":
+                        reasons.add(name)
+        os.unlink(self.path)
+        if sm:
+            out = {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax),
+                   "reasons": sorted(reasons), "samples": len(sm)}
+        return out
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline (reference build or oracle port), bounded sample
+# ---------------------------------------------------------------------------
+
+def cpu_lib_path():
+    ref = os.path.join(ROOT, "oracle", "_ref", "liborchard_ref.so")
+    if os.path.exists(ref):
+        return ref, "reference"
+    return os.path.join(ROOT, "oracle", "liborchard_oracle.so"), "port"
+
+
+def cpu_step_seconds(n_sample, steps=1):
+    """Seconds per projection step of the CPU implementation at n_sample^3."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    path, kind = cpu_lib_path()
+    lib = pyoracle.Oracle(path)
+    cfg = pyoracle.steps_config(n_sample, n_sample, n_sample, NU, CFL, steps, TOL, MAX_IT)
+    s = lib.tg_init(cfg, 0)
+    t0 = time.perf_counter()
+    lib.tg_steps(cfg, steps, s)
+    return (time.perf_counter() - t0) / steps, kind
+
+
+def _cpu_worker(args):
+    n_sample, steps = args
+    return cpu_step_seconds(n_sample, steps)[0]
+
+
+def cpu_baseline(n, n_sample=128):
+    sec, kind = cpu_step_seconds(n_sample, 1)
+    scale = (n_sample / n) ** 3
+    return {"value": scale / sec, "unit": "steps/s", "cores": 1, "kind": kind,
+            "sample": f"1 FP64 step of Taylor-Green {n_sample}^3 (nu=1/1600, CFL 0.5, tol 1e-12) "
+                      f"on 1 core took {sec:.2f} s; scaled by cell count to {n}^3",
+            "seconds_per_sample_step": sec}
+
+
+def run_reference_arm(args, world, rank):
+    """The reference's CPU step on all host cores (one process per core)."""
+    if rank != 0:
+        return 0
+    import multiprocessing as mp
+    cores = os.cpu_count() or 1
+    n_sample = args.cpu_sample_n
+    scale = (n_sample / args.n) ** 3
+    ctx = mp.get_context("spawn")
+    step_times = []
+    with ctx.Pool(cores) as pool:
+        for i in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            pool.map(_cpu_worker, [(n_sample, 1)] * cores)
+            dt = time.perf_counter() - t0
+            if i >= args.warmup:
+                step_times.append(dt)
+    per_step = sum(step_times) / len(step_times)
+    value = cores * scale / per_step
+    _, kind = cpu_lib_path()
+    sample = (f"each step: {cores} concurrent single-thread FP64 Taylor-Green {n_sample}^3 steps "
+              f"(nu=1/1600, CFL 0.5, tol 1e-12), scaled by cell count to {args.n}^3")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "steps/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 / value, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (analytic Taylor-Green)",
+        "config": {"workload": f"taylor_green_3d_{args.n}", "n": args.n, "viscosity": NU,
+                   "cfl": CFL, "poisson_tolerance": TOL},
+        "cpu_baseline": {"value": value, "unit": "steps/s", "cores": cores, "kind": kind,
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# B200 arm
+# ---------------------------------------------------------------------------
+
+def run_b200_arm(args, world, rank, local):
+    import numpy as np
+    import torch
+    import solver_b200 as sb
+
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    device = local
+
+    n = args.n
+    h = 2.0 * math.pi / n
+    grid = sb.Grid(n, n, n, h, h, h)
+    dt = tg_dt(n)
+    precision = sb.OF_MIXED if args.precision == "mixed" else sb.OF_FP64
+    ctx = sb.Context(grid, [sb.PERIODIC] * 6, device=device, precision=precision)
+    prm = sb.step_params(NU, dt, MAX_IT, TOL)
+    ctx.tg_init(NU, dt, mode=1)
+    stream = torch.cuda.ExternalStream(sb.context_stream(ctx), device=device)
+
+    def barrier():
+        if dist is not None:
+            t = torch.zeros(1, device=f"cuda:{device}")
+            dist.all_reduce(t)
+            torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{device}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        ctx.run_steps(prm, 1)
+
+    # ---- timed region: K steps on the resident state ----
+    sampler = ClockSampler(device)
+    sb.profile_reset()
+    sb.profile_enable(True)
+    barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    metrics = ctx.run_steps(prm, args.steps)
+    ev1.record(stream)
+    ev1.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    clocks = sampler.stop()
+    sb.profile_enable(False)
+    prof = sb.profile_read()
+    elapsed_ms = max_over_ranks(ev0.elapsed_time(ev1))
+    value = world * args.steps / (elapsed_ms / 1000.0)
+    launches = sum(v[0] for v in prof.values())
+
+    # ---- roofline of the dominant kernel class ----
+    bpl = bytes_per_launch(n, args.precision)
+    timed = {k: v for k, v in prof.items() if v[1] > 0 and k in bpl}
+    dom = max(timed, key=lambda k: timed[k][2])
+    dom_launches, dom_timed, dom_ms = timed[dom]
+    avg_s = dom_ms / dom_timed / 1000.0
+    achieved = bpl[dom] / avg_s / 1e9
+    peak, peak_kind = read_peaks()
+    traffic = read_traffic().get(dom)
+    step_bytes = sum(bpl[k] * v[0] for k, v in prof.items() if k in bpl) / args.steps
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                "traffic": traffic, "algorithmic_bytes_per_launch": bpl[dom],
+                "avg_launch_us": avg_s * 1e6, "launches": dom_launches,
+                "share_of_step": dom_ms / elapsed_ms}
+    step_hbm = {"algorithmic_bytes_per_step": step_bytes,
+                "achieved_gbs": step_bytes / (elapsed_ms / args.steps / 1000.0) / 1e9,
+                "frac": step_bytes / (elapsed_ms / args.steps / 1000.0) / 1e9 / peak}
+    kernels = {k: {"launches": v[0], "ms": round(v[2], 3)} for k, v in prof.items() if v[0]}
+
+    # ---- e2e: the C-ABI step call with host state in pinned memory ----
+    st = ctx.download_state()
+    pinned = {}
+    for k in ("u", "v", "w", "adv_u", "adv_v", "adv_w", "p"):
+        t = torch.empty(st[k].shape, dtype=torch.float64, pin_memory=True)
+        t.numpy()[...] = st[k]
+        pinned[k] = t.numpy()
+    state_bytes = sum(a.nbytes for a in pinned.values())
+    e2e_steps = max(1, min(args.steps, args.e2e_steps))
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        ctx.upload_state(pinned["u"], pinned["v"], pinned["w"], pinned["adv_u"], pinned["adv_v"],
+                         pinned["adv_w"], pinned["p"], 1, st["metrics"])
+        ctx.run_steps(prm, 1)
+        out = ctx.download_state_into(pinned)
+        st["metrics"] = out
+    e1.record(stream)
+    e1.synchronize()
+    barrier()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
+    e2e_value = world * e2e_steps / (e2e_ms / 1000.0)
+
+    line = {
+        "metric": METRIC if args.precision == "fp64" else METRIC.replace("FP64", "mixed FP32/FP64"),
+        "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f64+f32",
+        "data": "synthetic (analytic Taylor-Green initial state)",
+        "config": {"workload": f"taylor_green_3d_{n}", "n": n, "viscosity": NU, "cfl": CFL,
+                   "dt": dt, "poisson_tolerance": TOL, "precision": args.precision,
+                   "parallelism": f"replicas{world}", "l2": "every field > 126 MB L2; no flush",
+                   "pressure_iterations_last_step": metrics["pressure_iterations"]},
+        "roofline": roofline,
+        "step_hbm": step_hbm,
+        "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": state_bytes,
+                "d2h_bytes_per_step": state_bytes,
+                "note": "per step: state upload from pinned host memory, one step, state download "
+                        "(the C-ABI call a host-resident caller makes)"},
+        "gpu_launches": launches,
+        "clocks": clocks,
+        "kernels": kernels,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(n, args.cpu_sample_n)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist is not None:
+        barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--n", type=int, default=N_DEFAULT)
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-sample-n", type=int, default=None)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be at least 3")
+    if args.cpu_sample_n is None:
+        args.cpu_sample_n = 128 if args.impl == "b200" else 64
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        return run_reference_arm(args, world, rank)
+    return run_b200_arm(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -218,6 +218,21 @@ of_status of_tg_init(of_ctx* ctx, double viscosity, double dt, int mode);
 of_status of_run_steps(of_ctx* ctx, const of_step_params* params, int steps,
                        of_step_metrics* metrics);
 
+/* ---- instrumentation ---------------------------------------------------- */
+
+/* The context's CUDA stream (cudaStream_t) for callers that time on it. */
+of_status of_stream(of_ctx* ctx, void** stream);
+
+/* Kernel classes (predictor_rhs, adi_sweep, ..., see of_kernel_class_name).
+ * Every launch is counted; with profiling enabled each launch of a class is
+ * also bracketed by CUDA events on its stream and its device time summed. */
+int of_kernel_class_count(void);
+const char* of_kernel_class_name(int id);
+of_status of_profile_enable(int enable);
+of_status of_profile_reset(void);
+of_status of_profile_read(int id, long long* launches, long long* timed_launches,
+                          double* total_ms);
+
 #ifdef __cplusplus
 }
 #endif

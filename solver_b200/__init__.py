@@ -227,6 +227,18 @@ class Context:
                 "adv_w": arrs[5], "p": arrs[6], "has_previous_advection": hp.value,
                 "metrics": _struct_dict(m)}
 
+    def download_state_into(self, arrs):
+        """Downloads the resident state into caller arrays (dict of u, v, w,
+        adv_u, adv_v, adv_w, p); returns the step metrics."""
+        names = ("u", "v", "w", "adv_u", "adv_v", "adv_w", "p")
+        for name, loc in zip(names, "uvwuvwp"):
+            _check_shape(self.grid, arrs[name], loc, "download_state")
+        hp = C.c_int()
+        m = _capi.OfStepMetrics()
+        _capi.check(self._lib.of_state_download(self._h, *(_dp(arrs[k]) for k in names),
+                                                C.byref(hp), C.byref(m)))
+        return _struct_dict(m)
+
     def tg_init(self, viscosity, dt, mode=0):
         _capi.check(self._lib.of_tg_init(self._h, float(viscosity), float(dt), int(mode)))
 
@@ -245,3 +257,36 @@ def step_params(viscosity, dt, max_iterations, tolerance, variant=OF_CORRECTION_
                               float(tolerance), int(variant),
                               1 if variant == OF_CORRECTION_TAYLOR_GREEN else 0,
                               name.encode())
+
+
+# ---- instrumentation ---------------------------------------------------------
+
+def kernel_classes():
+    lib = _capi.load()
+    return [lib.of_kernel_class_name(i).decode() for i in range(lib.of_kernel_class_count())]
+
+
+def profile_enable(on=True):
+    _capi.check(_capi.load().of_profile_enable(1 if on else 0))
+
+
+def profile_reset():
+    _capi.check(_capi.load().of_profile_reset())
+
+
+def profile_read():
+    """{class name: (launches, timed launches, total device ms)}."""
+    lib = _capi.load()
+    out = {}
+    for i, name in enumerate(kernel_classes()):
+        n, t, ms = C.c_longlong(), C.c_longlong(), C.c_double()
+        _capi.check(lib.of_profile_read(i, C.byref(n), C.byref(t), C.byref(ms)))
+        out[name] = (n.value, t.value, ms.value)
+    return out
+
+
+def context_stream(ctx):
+    """The context's cudaStream_t as an integer handle."""
+    p = C.c_void_p()
+    _capi.check(ctx._lib.of_stream(ctx._h, C.byref(p)))
+    return p.value or 0

@@ -21,7 +21,8 @@ EXPORTED_SYMBOLS = (
     "of_abi_version", "of_last_error", "of_create", "of_destroy", "of_set_precision",
     "of_device_bytes", "of_compute_advection_term", "of_solve_predictor_adi",
     "of_solve_pressure_poisson", "of_project_velocity", "of_state_upload", "of_state_download",
-    "of_tg_init", "of_run_steps",
+    "of_tg_init", "of_run_steps", "of_stream", "of_kernel_class_count", "of_kernel_class_name",
+    "of_profile_enable", "of_profile_reset", "of_profile_read",
 )
 
 
@@ -107,6 +108,11 @@ def load():
         lib.of_tg_init.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int]
         lib.of_run_steps.argtypes = [C.c_void_p, C.POINTER(OfStepParams), C.c_int,
                                      C.POINTER(OfStepMetrics)]
+        lib.of_stream.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
+        lib.of_kernel_class_name.restype = C.c_char_p
+        lib.of_profile_enable.argtypes = [C.c_int]
+        lib.of_profile_read.argtypes = [C.c_int, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
+                                        C.POINTER(C.c_double)]
         _lib = lib
     return _lib
 

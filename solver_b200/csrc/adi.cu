@@ -275,6 +275,7 @@ void launch_adi_sweep(const AdiPlan* p, int comp, int axis, const double* in, do
   const int a2 = axis == 2 ? 1 : 2;
   dim3 block(128, 1, 1);
   dim3 grid((a.L.n(a1) + 127) / 128, a.L.n(a2), 1);
+  ProfScope ps(kKAdi, s);
   k_adi_sweep<<<grid, block, 0, s>>>(a, in, out);
   OFB_LAUNCH_CHECK("k_adi_sweep");
 }

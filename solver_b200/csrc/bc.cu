@@ -148,6 +148,7 @@ void launch_component_bc(const Grid& g, const VBC& bc, int comp, double* f, cuda
     dim3 grid((d1 + 31) / 32, (d2 + 7) / 8, 1);
     double* fs[3] = {nullptr, nullptr, nullptr};
     fs[comp] = f;
+    ProfScope ps(kKVelocityBc, s);
     k_velocity_bc_axis<<<grid, block, 0, s>>>(g, bc, axis, comp, fs[0], fs[1], fs[2]);
     OFB_LAUNCH_CHECK("k_velocity_bc_axis");
   }
@@ -163,6 +164,7 @@ void launch_velocity_bc(const Grid& g, const VBC& bc, double* u, double* v, doub
     const int d2 = (axis == 2 ? g.ny : g.nz) + 1;
     dim3 block(32, 8, 1);
     dim3 grid((d1 + 31) / 32, (d2 + 7) / 8, 3);
+    ProfScope ps(kKVelocityBc, s);
     k_velocity_bc_axis<<<grid, block, 0, s>>>(g, bc, axis, 0, u, v, w);
     OFB_LAUNCH_CHECK("k_velocity_bc_axis");
   }
@@ -175,6 +177,7 @@ void launch_total_pressure_bc(const Grid& g, const VBC& bc, double nu, const dou
   const int dm = d1 > d2 ? d1 : d2;
   dim3 block(32, 8, 1);
   dim3 grid((dm + 31) / 32, (dm + 7) / 8, 3);
+  ProfScope ps(kKTotalPressureBc, s);
   k_total_pressure_bc<<<grid, block, 0, s>>>(g, bc, nu, u, v, w, p);
   OFB_LAUNCH_CHECK("k_total_pressure_bc");
 }

@@ -343,6 +343,14 @@ of_status of_set_precision(of_ctx* ctx, int precision) {
   });
 }
 
+of_status of_stream(of_ctx* ctx, void** stream) {
+  return guarded([&] {
+    require_ctx(ctx);
+    require_ptr(stream, "stream");
+    *stream = static_cast<void*>(ctx->stream);
+  });
+}
+
 of_status of_device_bytes(of_ctx* ctx, size_t* bytes) {
   return guarded([&] {
     require_ctx(ctx);

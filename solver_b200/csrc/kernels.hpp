@@ -4,6 +4,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "prof.hpp"
 
 namespace ofb {
 

@@ -209,6 +209,7 @@ __global__ void k_tg_init(Grid g, int mode, int loc, double* f) {
 
 void launch_predictor_rhs(const PredictorArgs& a, cudaStream_t s) {
   const Lay Lu = make_lay(a.g, kFaceX), Lv = make_lay(a.g, kFaceY), Lw = make_lay(a.g, kFaceZ);
+  ProfScope ps(kKPredictor, s, 3);
   Launch3 l0 = launch3(Lu.nx, Lu.ny, Lu.nz);
   k_predictor_rhs<0><<<l0.grid, l0.block, 0, s>>>(a, l0.kchunk);
   OFB_LAUNCH_CHECK("k_predictor_rhs<0>");
@@ -223,6 +224,7 @@ void launch_predictor_rhs(const PredictorArgs& a, cudaStream_t s) {
 void launch_advection(const Grid& g, const double* u, const double* v, const double* w,
                       double* au, double* av, double* aw, cudaStream_t s) {
   const Lay Lu = make_lay(g, kFaceX), Lv = make_lay(g, kFaceY), Lw = make_lay(g, kFaceZ);
+  ProfScope ps(kKOther, s, 3);
   Launch3 l0 = launch3(Lu.nx, Lu.ny, Lu.nz);
   k_advection<0><<<l0.grid, l0.block, 0, s>>>(g, u, v, w, au, l0.kchunk);
   Launch3 l1 = launch3(Lv.nx, Lv.ny, Lv.nz);
@@ -240,6 +242,7 @@ void launch_tg_init(const Grid& g, int mode, double* u, double* v, double* w, do
     const Lay L = make_lay(g, loc);
     dim3 block(32, 8, 1);
     dim3 grid((L.nx + 31) / 32, (L.ny + 7) / 8, L.nz);
+    ProfScope ps(kKOther, s);
     k_tg_init<<<grid, block, 0, s>>>(g, mode, loc, f[loc]);
     OFB_LAUNCH_CHECK("k_tg_init");
   }

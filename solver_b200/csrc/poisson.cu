@@ -748,6 +748,7 @@ void v_cycle(PoissonPlan* P, int l, SolveScalars* sc, int first_rz, RedBuf rb, c
   T* a = static_cast<T*>(lv.a);
   T* x = static_cast<T*>(lv.x);
   if(l + 1 == nl) {
+    ProfScope ps(kKCoarseSolve, s);
     if(l == 0)
       k_coarse_solve<T, double><<<1, 256, 0, s>>>(P->coarse_n, P->swaps, P->factors, P->r, sb_ptr,
                                                   x, ls, zm, rz_sc, first_rz);
@@ -764,19 +765,35 @@ void v_cycle(PoissonPlan* P, int l, SolveScalars* sc, int first_rz, RedBuf rb, c
   LevelScalars* lsc = P->ls + (l + 1);
   auto smooth_chain = [&](auto* bptr) {
     using B = std::remove_cv_t<std::remove_pointer_t<decltype(bptr)>>;
-    k_smooth_first<T, B><<<ln.grid, ln.block, 0, s>>>(lv.op, bptr, sb_ptr, a, ls, zm, ln.kchunk, rb);
-    k_smooth<T, B><<<ln.grid, ln.block, 0, s>>>(lv.op, bptr, sb_ptr, a, &ls->sa, x, ls, 1, zm,
-                                                nullptr, 0, ln.kchunk, rb);
-    k_restrict_residual<T, B><<<lc.grid, lc.block, 0, s>>>(lv.op, cv.op, bptr, sb_ptr, x, &ls->sx,
+    const bool fine = l == 0;
+    {
+      ProfScope ps(fine ? kKSmoothFirstFine : kKCoarseLevels, s);
+      k_smooth_first<T, B><<<ln.grid, ln.block, 0, s>>>(lv.op, bptr, sb_ptr, a, ls, zm, ln.kchunk, rb);
+    }
+    {
+      ProfScope ps(fine ? kKSmoothFine : kKCoarseLevels, s);
+      k_smooth<T, B><<<ln.grid, ln.block, 0, s>>>(lv.op, bptr, sb_ptr, a, &ls->sa, x, ls, 1, zm,
+                                                  nullptr, 0, ln.kchunk, rb);
+    }
+    {
+      ProfScope ps(fine ? kKRestrictFine : kKCoarseLevels, s);
+      k_restrict_residual<T, B><<<lc.grid, lc.block, 0, s>>>(lv.op, cv.op, bptr, sb_ptr, x, &ls->sx,
                                                            static_cast<T*>(cv.b), lsc, lv.rx,
                                                            lv.ry, lv.rz, zm, lc.kchunk, rb);
+    }
     OFB_LAUNCH_CHECK("v_cycle descent");
     v_cycle<T>(P, l + 1, sc, first_rz, rb, s);
-    k_prolong_smooth<T, B><<<ln.grid, ln.block, 0, s>>>(lv.op, cv.L, bptr, sb_ptr, x, &ls->sx,
-                                                        static_cast<const T*>(cv.x), &lsc->sx, a,
-                                                        ls, lv.rx, lv.ry, lv.rz, zm, ln.kchunk, rb);
-    k_smooth<T, B><<<ln.grid, ln.block, 0, s>>>(lv.op, bptr, sb_ptr, a, &ls->sa, x, ls, 1, zm,
-                                                rz_sc, first_rz, ln.kchunk, rb);
+    {
+      ProfScope ps(fine ? kKProlongFine : kKCoarseLevels, s);
+      k_prolong_smooth<T, B><<<ln.grid, ln.block, 0, s>>>(lv.op, cv.L, bptr, sb_ptr, x, &ls->sx,
+                                                          static_cast<const T*>(cv.x), &lsc->sx, a,
+                                                          ls, lv.rx, lv.ry, lv.rz, zm, ln.kchunk, rb);
+    }
+    {
+      ProfScope ps(fine ? kKSmoothFine : kKCoarseLevels, s);
+      k_smooth<T, B><<<ln.grid, ln.block, 0, s>>>(lv.op, bptr, sb_ptr, a, &ls->sa, x, ls, 1, zm,
+                                                  rz_sc, first_rz, ln.kchunk, rb);
+    }
     OFB_LAUNCH_CHECK("v_cycle ascent");
   };
   if(l == 0) smooth_chain(static_cast<const double*>(P->r));
@@ -803,7 +820,10 @@ void solve_impl(PoissonPlan* P, int max_iterations, double tolerance, SolveScala
   }
   init.sp = 0.0;
   OFB_CHECK(cudaMemcpyAsync(sc, &init, sizeof(SolveScalars), cudaMemcpyHostToDevice, s));
-  k_initial_residual<<<ln.grid, ln.block, 0, s>>>(l0.op, P->b, P->x, P->r, sc, ln.kchunk, rb);
+  {
+    ProfScope ps(kKInitResidual, s);
+    k_initial_residual<<<ln.grid, ln.block, 0, s>>>(l0.op, P->b, P->x, P->r, sc, ln.kchunk, rb);
+  }
   OFB_LAUNCH_CHECK("k_initial_residual");
   OFB_CHECK(cudaMemcpyAsync(host, sc, sizeof(SolveScalars), cudaMemcpyDeviceToHost, s));
   OFB_CHECK(cudaStreamSynchronize(s));
@@ -812,12 +832,21 @@ void solve_impl(PoissonPlan* P, int max_iterations, double tolerance, SolveScala
   ++nh;
   if(host->converged) return;
   v_cycle<T>(P, 0, sc, 1, rb, s);
-  k_update_p<T><<<ln.grid, ln.block, 0, s>>>(l0.L, static_cast<const T*>(l0.x), P->ls, P->p, sc, 1,
-                                             ln.kchunk, rb);
+  {
+    ProfScope ps(kKUpdateP, s);
+    k_update_p<T><<<ln.grid, ln.block, 0, s>>>(l0.L, static_cast<const T*>(l0.x), P->ls, P->p, sc, 1,
+                                               ln.kchunk, rb);
+  }
   OFB_LAUNCH_CHECK("k_update_p");
   for(int it = 0; it < max_iterations; ++it) {
-    k_apply_ap<<<ln.grid, ln.block, 0, s>>>(l0.op, P->p, P->ap, sc, ln.kchunk, rb);
-    k_update_xr<<<ln.grid, ln.block, 0, s>>>(l0.L, P->x, P->r, P->p, P->ap, sc, ln.kchunk, rb);
+    {
+      ProfScope ps(kKApplyAp, s);
+      k_apply_ap<<<ln.grid, ln.block, 0, s>>>(l0.op, P->p, P->ap, sc, ln.kchunk, rb);
+    }
+    {
+      ProfScope ps(kKUpdateXr, s);
+      k_update_xr<<<ln.grid, ln.block, 0, s>>>(l0.L, P->x, P->r, P->p, P->ap, sc, ln.kchunk, rb);
+    }
     OFB_LAUNCH_CHECK("k_update_xr");
     OFB_CHECK(cudaMemcpyAsync(host, sc, sizeof(SolveScalars), cudaMemcpyDeviceToHost, s));
     OFB_CHECK(cudaStreamSynchronize(s));
@@ -826,8 +855,11 @@ void solve_impl(PoissonPlan* P, int max_iterations, double tolerance, SolveScala
     ++nh;
     if(host->converged) break;
     v_cycle<T>(P, 0, sc, 0, rb, s);
-    k_update_p<T><<<ln.grid, ln.block, 0, s>>>(l0.L, static_cast<const T*>(l0.x), P->ls, P->p, sc,
-                                               0, ln.kchunk, rb);
+    {
+      ProfScope ps(kKUpdateP, s);
+      k_update_p<T><<<ln.grid, ln.block, 0, s>>>(l0.L, static_cast<const T*>(l0.x), P->ls, P->p, sc,
+                                                 0, ln.kchunk, rb);
+    }
     OFB_LAUNCH_CHECK("k_update_p");
   }
 }
@@ -849,6 +881,7 @@ void launch_compact_to_pressure(const Grid& g, const double* x, const SolveScala
                                 double* p_padded, cudaStream_t s) {
   dim3 block(32, 8, 1);
   dim3 grid((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz);
+  ProfScope ps(kKOther, s);
   k_compact_to_pressure<<<grid, block, 0, s>>>(g, x, sc, p_padded);
   OFB_LAUNCH_CHECK("k_compact_to_pressure");
 }

@@ -1,0 +1,44 @@
+// Kernel classes for launch accounting and event timing (prof.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace ofb {
+
+enum KernelClass : int {
+  kKPredictor = 0,
+  kKAdi,
+  kKVelocityBc,
+  kKDivergence,
+  kKInitResidual,
+  kKApplyAp,
+  kKUpdateXr,
+  kKUpdateP,
+  kKSmoothFirstFine,
+  kKSmoothFine,
+  kKRestrictFine,
+  kKProlongFine,
+  kKCoarseLevels,
+  kKCoarseSolve,
+  kKCorrect,
+  kKCellPass,
+  kKTotalPressureBc,
+  kKOther,
+  kKernelCount
+};
+
+void prof_launch(int id, cudaStream_t s, bool begin, int count = 1);
+void prof_collect();
+
+// Brackets `count` kernel launches of one class: counts them and, when timing
+// is on, records an event pair around them on their stream.
+struct ProfScope {
+  int id;
+  cudaStream_t s;
+  ProfScope(int id_, cudaStream_t s_, int count = 1) : id(id_), s(s_) {
+    prof_launch(id, s, true, count);
+  }
+  ~ProfScope() { prof_launch(id, s, false); }
+};
+
+}  // namespace ofb

@@ -241,6 +241,7 @@ void launch_divergence_rhs(const Grid& g, const PBC& pbc, const double* u, const
       with_source = 1;
   }
   const Launch3 l = launch3(g.nx, g.ny, g.nz);
+  ProfScope ps(kKDivergence, s);
   k_divergence_rhs<<<l.grid, l.block, 0, s>>>(g, pbc, u, v, w, scale, rhs_padded, b, sc, zm,
                                               with_source, l.kchunk, rb);
   OFB_LAUNCH_CHECK("k_divergence_rhs");
@@ -252,6 +253,7 @@ void launch_rhs_to_system(const Grid& g, const PBC& pbc, const double* rhs_padde
   for(int f = 0; f < 6; ++f)
     if(pbc.type[f] == kPDirichlet) zm = 0;
   const Launch3 l = launch3(g.nx, g.ny, g.nz);
+  ProfScope ps(kKOther, s);
   k_rhs_to_system<<<l.grid, l.block, 0, s>>>(g, pbc, rhs_padded, b, sc, zm, l.kchunk, rb);
   OFB_LAUNCH_CHECK("k_rhs_to_system");
 }
@@ -259,6 +261,7 @@ void launch_rhs_to_system(const Grid& g, const PBC& pbc, const double* rhs_padde
 void launch_pressure_to_compact(const Grid& g, const double* p_padded, double* x,
                                 SolveScalars* sc, int zm, RedBuf rb, cudaStream_t s) {
   const Launch3 l = launch3(g.nx, g.ny, g.nz);
+  ProfScope ps(kKOther, s);
   k_pressure_to_compact<<<l.grid, l.block, 0, s>>>(g, p_padded, x, sc, zm, l.kchunk, rb);
   OFB_LAUNCH_CHECK("k_pressure_to_compact");
 }
@@ -269,6 +272,7 @@ void launch_correct_velocity(const Grid& g, const PBC& pbc, const double* x,
                              const double* prev_u, const double* prev_v, const double* prev_w,
                              SolveScalars* sc_out, RedBuf rb, cudaStream_t s) {
   const Lay Lu = make_lay(g, kFaceX), Lv = make_lay(g, kFaceY), Lw = make_lay(g, kFaceZ);
+  ProfScope ps(kKCorrect, s, 3);
   const Launch3 l0 = launch3(Lu.nx, Lu.ny, Lu.nz);
   k_correct<0><<<l0.grid, l0.block, 0, s>>>(g, pbc, x, sc, pu, scale, cu, prev_u, sc_out,
                                             l0.kchunk, rb);
@@ -283,6 +287,7 @@ void launch_correct_velocity(const Grid& g, const PBC& pbc, const double* x,
 
 void launch_cell_pass(const CellPassArgs& a, SolveScalars* sc, RedBuf rb, cudaStream_t s) {
   const Launch3 l = launch3(a.g.nx, a.g.ny, a.g.nz);
+  ProfScope ps(kKCellPass, s);
   k_cell_pass<<<l.grid, l.block, 0, s>>>(a, sc, l.kchunk, rb);
   OFB_LAUNCH_CHECK("k_cell_pass");
 }
