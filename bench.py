@@ -158,6 +158,21 @@ class ClockSampler:
         return out
 
 
+def reduce_max(x, dist, device=None):
+    """Max of a per-rank scalar over all ranks (identity without a process group)."""
+    if dist is None or not dist.is_initialized():
+        return x
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device or "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(steps_per_rank, elapsed_ms_max, world):
+    """Whole-job steps/s of `world` independent replicas timed as the max over ranks."""
+    return world * steps_per_rank / (elapsed_ms_max / 1000.0)
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -276,11 +291,7 @@ def run_b200_arm(args, world, rank, local):
             torch.cuda.synchronize()
 
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{device}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(x, dist, f"cuda:{device}")
 
     for _ in range(args.warmup):
         ctx.run_steps(prm, 1)
@@ -304,7 +315,7 @@ def run_b200_arm(args, world, rank, local):
     sb.profile_enable(False)
     prof = sb.profile_read()
     elapsed_ms = max_over_ranks(ev0.elapsed_time(ev1))
-    value = world * args.steps / (elapsed_ms / 1000.0)
+    value = replica_throughput(args.steps, elapsed_ms, world)
     launches = sum(v[0] for v in prof.values())
 
     # ---- roofline of the dominant kernel class ----
@@ -351,7 +362,7 @@ def run_b200_arm(args, world, rank, local):
     e1.synchronize()
     barrier()
     e2e_ms = max_over_ranks(e0.elapsed_time(e1))
-    e2e_value = world * e2e_steps / (e2e_ms / 1000.0)
+    e2e_value = replica_throughput(e2e_steps, e2e_ms, world)
 
     line = {
         "metric": METRIC if args.precision == "fp64" else METRIC.replace("FP64", "mixed FP32/FP64"),

@@ -1636,6 +1636,58 @@ int oo_tg_steps(const oo_tg_config* c, int steps, oo_state* s) {
   return run_steps(&D, steps, s, 1);
 }
 
+/* kinetic_energy / exact_* / velocity_relative_l2_error / build_validation
+ * (solver/taylor_green.cpp:258-333, 403-417) */
+int oo_tg_validate(const oo_tg_config* c, int mode, const double* u, const double* v,
+                   const double* w, double time, oo_tg_validation* out) {
+  oo_grid g;
+  int rc = oo_tg_grid(c, &g);
+  if(rc) return rc;
+  int three_d = c->nz > 1;
+  lay_t P = layout_of(&g, LOC_CELL);
+  lay_t U = layout_of(&g, LOC_FX), V = layout_of(&g, LOC_FY), W = layout_of(&g, LOC_FZ);
+  double energy_sum = 0.0;
+  size_t count = 0;
+  FOR_ACTIVE(&P) {
+    double uc = 0.5 * (u[IDX(&U, i, j, k)] + u[IDX(&U, i + 1, j, k)]);
+    double vc = 0.5 * (v[IDX(&V, i, j, k)] + v[IDX(&V, i, j + 1, k)]);
+    double wc = 0.5 * (w[IDX(&W, i, j, k)] + w[IDX(&W, i, j, k + 1)]);
+    energy_sum += 0.5 * (uc * uc + vc * vc + wc * wc);
+    ++count;
+  }
+  double ke = energy_sum / (double)count;
+  double exact = (three_d ? 0.125 : 0.25) * exp(-(three_d ? 6.0 : 4.0) * c->viscosity * time);
+  double decay = exp(-(three_d ? 3.0 : 2.0) * c->viscosity * time);
+  double num = 0.0, den = 0.0;
+  FOR_ACTIVE(&U) {
+    double z = coord(&U, AZ, k), y = coord(&U, AY, j), x = coord(&U, AX, i);
+    double ref;
+    if(mode == 0) ref = three_d ? -cos(x) * sin(y) * cos(z) * decay : -cos(x) * sin(y) * decay;
+    else ref = three_d ? sin(x) * cos(y) * cos(z) * decay : sin(x) * cos(y) * decay;
+    double d = u[IDX(&U, i, j, k)] - ref;
+    num += d * d;
+    den += ref * ref;
+  }
+  FOR_ACTIVE(&V) {
+    double z = coord(&V, AZ, k), y = coord(&V, AY, j), x = coord(&V, AX, i);
+    double ref;
+    if(mode == 0) ref = three_d ? sin(x) * cos(y) * cos(z) * decay : sin(x) * cos(y) * decay;
+    else ref = three_d ? -cos(x) * sin(y) * cos(z) * decay : -cos(x) * sin(y) * decay;
+    double d = v[IDX(&V, i, j, k)] - ref;
+    num += d * d;
+    den += ref * ref;
+  }
+  FOR_ACTIVE(&W) {
+    double d = w[IDX(&W, i, j, k)];
+    num += d * d;
+  }
+  out->kinetic_energy = ke;
+  out->exact_kinetic_energy = exact;
+  out->normalized_energy_error = fabs(ke - exact) / exact;
+  out->velocity_relative_l2_error = den > 0.0 ? sqrt(num / den) : sqrt(num);
+  return OK;
+}
+
 /* ---- lid-driven cavity (solver/lid_driven_cavity.cpp) ---- */
 
 static int cavity_validate(const oo_cavity_config* c) {

@@ -179,6 +179,18 @@ int oo_tg_init(const oo_tg_config* c, int mode, oo_state* s);
  * velocity BC, diffusion, total-pressure BC (solver/taylor_green.cpp:391-394). */
 int oo_tg_init_tail(const oo_tg_config* c, oo_state* s);
 int oo_tg_steps(const oo_tg_config* c, int steps, oo_state* s);
+/* Validation of finalize_taylor_green_result (solver/taylor_green.cpp:258-333,
+ * 403-417): kinetic energy, exact kinetic energy at `time`, normalized energy
+ * error and velocity relative L2 error against the analytic decay.  mode as
+ * in oo_tg_init (the analytic field is shifted the same way). */
+typedef struct {
+  double kinetic_energy;
+  double exact_kinetic_energy;
+  double normalized_energy_error;
+  double velocity_relative_l2_error;
+} oo_tg_validation;
+int oo_tg_validate(const oo_tg_config* c, int mode, const double* u, const double* v,
+                   const double* w, double time, oo_tg_validation* out);
 
 /* Lid-driven cavity driver (solver/lid_driven_cavity.cpp:339-624). */
 int oo_cavity_grid(const oo_cavity_config* c, oo_grid* g);

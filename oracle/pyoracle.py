@@ -81,6 +81,12 @@ class TGConfig(C.Structure):
                 ("poisson_max_iterations", C.c_int), ("poisson_tolerance", C.c_double)]
 
 
+class TGValidation(C.Structure):
+    _fields_ = [("kinetic_energy", C.c_double), ("exact_kinetic_energy", C.c_double),
+                ("normalized_energy_error", C.c_double),
+                ("velocity_relative_l2_error", C.c_double)]
+
+
 class CavityConfig(C.Structure):
     _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("reynolds", C.c_double),
                 ("lid_velocity", C.c_double), ("cfl_limit", C.c_double), ("max_steps", C.c_int),
@@ -279,6 +285,14 @@ class Oracle:
         self._check(self.lib.oo_tg_steps(C.byref(cfg), steps, C.byref(cs)))
         s.from_c(cs)
         return s
+
+    def tg_validate(self, cfg, s_or_fields, time, mode=0):
+        u, v, w = (s_or_fields.u, s_or_fields.v, s_or_fields.w) if hasattr(s_or_fields, "u") \
+            else s_or_fields
+        out = TGValidation()
+        self._check(self.lib.oo_tg_validate(C.byref(cfg), mode, ptr(u), ptr(v), ptr(w),
+                                            C.c_double(time), C.byref(out)))
+        return {k: getattr(out, k) for k, _ in TGValidation._fields_}
 
     # --- cavity -------------------------------------------------------------
     def cavity_grid(self, cfg):

@@ -445,6 +445,25 @@ int oo_tg_steps(const oo_tg_config* c, int steps, oo_state* s) {
   });
 }
 
+int oo_tg_validate(const oo_tg_config* c, int mode, const double* u, const double* v,
+                   const double* w, double time, oo_tg_validation* out) {
+  return guarded([&] {
+    if(mode != 0) {
+      throw std::invalid_argument("the reference validates its own initial state only (mode 0)");
+    }
+    solver::TaylorGreenConfig config = make_tg(c);
+    config.validate_energy = true;
+    solver::TaylorGreenState st(solver::make_taylor_green_grid(config));
+    load_velocity(st.velocity, u, v, w);
+    st.metrics.time = time;
+    const solver::TaylorGreenResult r = solver::finalize_taylor_green_result(config, st);
+    out->kinetic_energy = r.final_kinetic_energy;
+    out->exact_kinetic_energy = r.validation.exact_kinetic_energy;
+    out->normalized_energy_error = r.validation.normalized_energy_error;
+    out->velocity_relative_l2_error = r.validation.velocity_relative_l2_error;
+  });
+}
+
 int oo_cavity_grid(const oo_cavity_config* c, oo_grid* g) {
   return guarded([&] {
     const solver::Grid grid = solver::make_lid_driven_cavity_grid(make_cavity(c));
