@@ -296,10 +296,9 @@ def run_b200_arm(args, world, rank, local):
     for _ in range(args.warmup):
         ctx.run_steps(prm, 1)
 
-    # ---- timed region: K steps on the resident state ----
+    # ---- timed region: K steps on the resident state (no instrumentation) ----
     sampler = ClockSampler(device)
     sb.profile_reset()
-    sb.profile_enable(True)
     barrier()
     torch.cuda.synchronize()
     sampler.start()
@@ -312,11 +311,26 @@ def run_b200_arm(args, world, rank, local):
     torch.cuda.synchronize()
     barrier()
     clocks = sampler.stop()
-    sb.profile_enable(False)
-    prof = sb.profile_read()
+    counted = sb.profile_read()
+    launches = sum(v[0] for v in counted.values())
     elapsed_ms = max_over_ranks(ev0.elapsed_time(ev1))
     value = replica_throughput(args.steps, elapsed_ms, world)
-    launches = sum(v[0] for v in prof.values())
+
+    # ---- per-kernel device times: the same steps replayed with every launch
+    # bracketed by CUDA events on the context stream (kernels launched one by
+    # one, so the event pairs see each kernel alone) ----
+    replay_steps = max(1, min(args.steps, args.profile_steps))
+    sb.profile_reset()
+    sb.profile_enable(True)
+    pr0 = torch.cuda.Event(enable_timing=True)
+    pr1 = torch.cuda.Event(enable_timing=True)
+    pr0.record(stream)
+    ctx.run_steps(prm, replay_steps)
+    pr1.record(stream)
+    pr1.synchronize()
+    sb.profile_enable(False)
+    prof = sb.profile_read()
+    replay_ms = pr0.elapsed_time(pr1)
 
     # ---- roofline of the dominant kernel class ----
     bpl = bytes_per_launch(n, args.precision)
@@ -327,16 +341,19 @@ def run_b200_arm(args, world, rank, local):
     achieved = bpl[dom] / avg_s / 1e9
     peak, peak_kind = read_peaks()
     traffic = read_traffic().get(dom)
-    step_bytes = sum(bpl[k] * v[0] for k, v in prof.items() if k in bpl) / args.steps
+    step_bytes = sum(bpl[k] * v[0] for k, v in prof.items() if k in bpl) / replay_steps
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                 "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
                 "traffic": traffic, "algorithmic_bytes_per_launch": bpl[dom],
-                "avg_launch_us": avg_s * 1e6, "launches": dom_launches,
-                "share_of_step": dom_ms / elapsed_ms}
+                "avg_launch_us": avg_s * 1e6, "launches_per_step": dom_launches / replay_steps,
+                "share_of_replay": dom_ms / replay_ms,
+                "timing": "CUDA events around each launch, instrumented replay of "
+                          f"{replay_steps} of the timed steps"}
     step_hbm = {"algorithmic_bytes_per_step": step_bytes,
                 "achieved_gbs": step_bytes / (elapsed_ms / args.steps / 1000.0) / 1e9,
                 "frac": step_bytes / (elapsed_ms / args.steps / 1000.0) / 1e9 / peak}
-    kernels = {k: {"launches": v[0], "ms": round(v[2], 3)} for k, v in prof.items() if v[0]}
+    kernels = {k: {"launches_per_step": v[0] / replay_steps, "ms_per_step": round(v[2] / replay_steps, 4)}
+               for k, v in prof.items() if v[0]}
 
     # ---- e2e: the C-ABI step call with host state in pinned memory ----
     st = ctx.download_state()
@@ -405,6 +422,7 @@ def main():
     ap.add_argument("--n", type=int, default=N_DEFAULT)
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--profile-steps", type=int, default=2)
     ap.add_argument("--cpu-sample-n", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

@@ -29,6 +29,13 @@ struct SolveScalars {
   double div_before_l2, div_after_l2, rhs_l2;
   double max_cfl, max_dv;
   int nonfinite;
+  // loop control of the rotated CG loop (one body = V-cycle, p, A p, x/r)
+  int first;      // the next p update is the first (p = z)
+  int max_it;
+  int cont;       // run another body
+  int body_runs;
+  double* hist;   // device residual history, hist[0] = r0
+  int hist_cap;
 };
 
 // Per-level mean shifts of the V-cycle vectors.

@@ -20,9 +20,12 @@
 // storage type T is double (OF_FP64) or float (OF_MIXED: FP32 storage and
 // arithmetic inside the FP64 CG loop).
 #include "kernels.hpp"
+#include "vstencil.cuh"
 
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
+#include <algorithm>
 #include <type_traits>
 #include <vector>
 
@@ -51,28 +54,56 @@ __device__ __forceinline__ double inv_diag(const OpInfo& o, int i, int j, int k)
   return __ldg(&o.invd[t]);
 }
 
-// apply_poisson_operator at (i, j, k) with homogeneous boundary rules
-// (neighbor_value, linsolve/poisson_solver.cpp:195-242): periodic wrap,
-// Neumann ghost = centre, Dirichlet ghost = -centre.  val(i, j, k) returns the
-// operand at an in-range cell.
+// Neighbour coordinates along one axis, branch-free: the in-range neighbour,
+// the periodic image, or the cell itself with sign +1 (homogeneous Neumann,
+// ghost = centre) or -1 (homogeneous Dirichlet, ghost = -centre)
+// (neighbor_value, linsolve/poisson_solver.cpp:195-242).  Every load is then
+// unconditional and in bounds, so a thread can keep many loads in flight.
+__device__ __forceinline__ void nb_lo(int c, int n, int per, int dir, int& cc, double& sg) {
+  const bool in = c > 0;
+  cc = in ? c - 1 : (per ? n - 1 : c);
+  sg = (in || per || !dir) ? 1.0 : -1.0;
+}
+
+__device__ __forceinline__ void nb_hi(int c, int n, int per, int dir, int& cc, double& sg) {
+  const bool in = c < n - 1;
+  cc = in ? c + 1 : (per ? 0 : c);
+  sg = (in || per || !dir) ? 1.0 : -1.0;
+}
+
+// In-plane neighbours of one (i, j) column; fixed while the thread marches in k.
+struct ColNb {
+  int xl, xr, yd, yu;
+  double sxl, sxr, syd, syu;
+};
+
+__device__ __forceinline__ ColNb col_nb(const OpInfo& o, int i, int j) {
+  ColNb c;
+  nb_lo(i, o.L.nx, o.periodic[0], o.dir_lo[0], c.xl, c.sxl);
+  nb_hi(i, o.L.nx, o.periodic[0], o.dir_hi[0], c.xr, c.sxr);
+  nb_lo(j, o.L.ny, o.periodic[1], o.dir_lo[1], c.yd, c.syd);
+  nb_hi(j, o.L.ny, o.periodic[1], o.dir_hi[1], c.yu, c.syu);
+  return c;
+}
+
+// apply_poisson_operator at (i, j, k) (linsolve/poisson_solver.cpp:244-269):
+// -(r - 2c + l)/dx^2 - (u - 2c + d)/dy^2 - (f - 2c + b)/dz^2 with the boundary
+// rules above.  val(i, j, k) returns the operand at an in-range cell.
 template <typename A, typename F>
-__device__ __forceinline__ A apply_op(const OpInfo& o, int i, int j, int k, F val, A& center) {
-  const CLay& L = o.L;
+__device__ __forceinline__ A apply_op(const OpInfo& o, const ColNb& nb, int i, int j, int k, F val,
+                                      A& center) {
+  int kb, kf;
+  double sb, sf;
+  nb_lo(k, o.L.nz, o.periodic[2], o.dir_lo[2], kb, sb);
+  nb_hi(k, o.L.nz, o.periodic[2], o.dir_hi[2], kf, sf);
   const A c = val(i, j, k);
+  const A l = A(nb.sxl) * val(nb.xl, j, k);
+  const A r = A(nb.sxr) * val(nb.xr, j, k);
+  const A d = A(nb.syd) * val(i, nb.yd, k);
+  const A u = A(nb.syu) * val(i, nb.yu, k);
+  const A b = A(sb) * val(i, j, kb);
+  const A f = A(sf) * val(i, j, kf);
   center = c;
-  A l, r, d, u, b, f;
-  if(i > 0) l = val(i - 1, j, k);
-  else l = o.periodic[0] ? val(L.nx - 1, j, k) : (o.dir_lo[0] ? -c : c);
-  if(i < L.nx - 1) r = val(i + 1, j, k);
-  else r = o.periodic[0] ? val(0, j, k) : (o.dir_hi[0] ? -c : c);
-  if(j > 0) d = val(i, j - 1, k);
-  else d = o.periodic[1] ? val(i, L.ny - 1, k) : (o.dir_lo[1] ? -c : c);
-  if(j < L.ny - 1) u = val(i, j + 1, k);
-  else u = o.periodic[1] ? val(i, 0, k) : (o.dir_hi[1] ? -c : c);
-  if(k > 0) b = val(i, j, k - 1);
-  else b = o.periodic[2] ? val(i, j, L.nz - 1) : (o.dir_lo[2] ? -c : c);
-  if(k < L.nz - 1) f = val(i, j, k + 1);
-  else f = o.periodic[2] ? val(i, j, 0) : (o.dir_hi[2] ? -c : c);
   const A two_c = A(2) * c;
   return -(r - two_c + l) * A(o.inv2[0]) - (u - two_c + d) * A(o.inv2[1]) -
          (f - two_c + b) * A(o.inv2[2]);
@@ -84,12 +115,37 @@ __device__ __forceinline__ void zero(double (&v)[K]) {
   for(int q = 0; q < K; ++q) v[q] = 0.0;
 }
 
+// Marches k in [k0, k1) in batches of KB planes: compute(k) holds only loads
+// and arithmetic, commit(k, r) the stores and reductions, so the loads of a
+// whole batch are independent and issued together.
+constexpr int kBatch = 4;
+
+template <int KB, typename Compute, typename Commit>
+__device__ __forceinline__ void k_batched(int k0, int k1, Compute compute, Commit commit) {
+  using R = decltype(compute(0));
+  int k = k0;
+  for(; k + KB <= k1; k += KB) {
+    R r[KB];
+#pragma unroll
+    for(int t = 0; t < KB; ++t) r[t] = compute(k + t);
+#pragma unroll
+    for(int t = 0; t < KB; ++t) commit(k + t, r[t]);
+  }
+  for(; k < k1; ++k) commit(k, compute(k));
+}
+
 #define STENCIL_PROLOGUE(L)                                 \
   const int i = blockIdx.x * kTX + threadIdx.x;             \
   const int j = blockIdx.y * kTY + threadIdx.y;             \
   const bool valid = i < (L).nx && j < (L).ny;              \
   const int k0 = blockIdx.z * kchunk;                       \
   const int k1 = min(k0 + kchunk, (L).nz);
+
+template <typename A>
+struct Pair {
+  A v;
+  double w;
+};
 
 // ---------------------------------------------------------------------------
 // V-cycle kernels.  Level vectors are T; shifts and scalars are double.
@@ -106,12 +162,14 @@ __global__ void __launch_bounds__(kTX* kTY)
   double acc[1];
   zero(acc);
   if(valid) {
-    for(int k = k0; k < k1; ++k) {
-      const int q = o.L.idx(i, j, k);
-      const A v = A(kOmega) * A(double(b[q]) - sb) * A(inv_diag(o, i, j, k));
-      a[q] = T(v);
-      acc[0] += double(v);
-    }
+    const A om = A(kOmega);
+    k_batched<kBatch>(
+        k0, k1,
+        [&](int k) { return om * A(double(b[o.L.idx(i, j, k)]) - sb) * A(inv_diag(o, i, j, k)); },
+        [&](int k, A v) {
+          a[o.L.idx(i, j, k)] = T(v);
+          acc[0] += double(v);
+        });
   }
   const bool mx[1] = {false};
   const int n = o.L.count();
@@ -121,12 +179,12 @@ __global__ void __launch_bounds__(kTX* kTY)
 // Jacobi sweep (smooth_jacobi, linsolve/poisson_solver.cpp:569-595):
 // out = x + omega (b - sb - A x) / D with x = in - s_in; records mean(out).
 // `which` selects the LevelScalars slot for the output mean (0: sa, 1: sx).
-// For the finest level with rz != nullptr, also accumulates (b - sb) . out.
+// On the finest level with sc != nullptr it also forms r.z for the CG.
 template <typename T, typename B>
 __global__ void __launch_bounds__(kTX* kTY)
     k_smooth(OpInfo o, const B* __restrict__ b, const double* sb_ptr, const T* __restrict__ in,
              const double* sin_ptr, T* __restrict__ out, LevelScalars* ls, int which, int zm,
-             SolveScalars* sc, int first_rz, int kchunk, RedBuf rb) {
+             SolveScalars* sc, int kchunk, RedBuf rb) {
   STENCIL_PROLOGUE(o.L)
   using A = T;
   const double sb = *sb_ptr;
@@ -134,17 +192,22 @@ __global__ void __launch_bounds__(kTX* kTY)
   double acc[2];
   zero(acc);
   if(valid) {
-    for(int k = k0; k < k1; ++k) {
-      const int q = o.L.idx(i, j, k);
-      A c;
-      const A ax = apply_op<A>(o, i, j, k,
-                               [&](int ii, int jj, int kk) { return A(in[o.L.idx(ii, jj, kk)]) - sin; }, c);
-      const double bq = double(b[q]) - sb;
-      const A v = c + A(kOmega) * (A(bq) - ax) * A(inv_diag(o, i, j, k));
-      out[q] = T(v);
-      acc[0] += double(v);
-      acc[1] += bq * double(v);
-    }
+    const ColNb nb = col_nb(o, i, j);
+    const A om = A(kOmega);
+    auto val = [&](int ii, int jj, int kk) { return A(in[o.L.idx(ii, jj, kk)]) - sin; };
+    k_batched<kBatch>(
+        k0, k1,
+        [&](int k) {
+          A c;
+          const A ax = apply_op<A>(o, nb, i, j, k, val, c);
+          const double bq = double(b[o.L.idx(i, j, k)]) - sb;
+          return Pair<A>{c + om * (A(bq) - ax) * A(inv_diag(o, i, j, k)), bq};
+        },
+        [&](int k, Pair<A> r) {
+          out[o.L.idx(i, j, k)] = T(r.v);
+          acc[0] += double(r.v);
+          acc[1] += r.w * double(r.v);
+        });
   }
   const bool mx[2] = {false, false};
   const int n = o.L.count();
@@ -158,7 +221,7 @@ __global__ void __launch_bounds__(kTX* kTY)
     if(sc != nullptr) {
       // r.z with z = out - mean (linsolve/poisson_solver.cpp:749, :791)
       const double rz_new = s.v[1] - mean * (sc->sum_r - sc->n * sc->sr);
-      if(first_rz) {
+      if(sc->first) {
         sc->rz = rz_new;
       } else {
         sc->beta = rz_new / sc->rz;
@@ -170,34 +233,48 @@ __global__ void __launch_bounds__(kTX* kTY)
 
 // Residual + restriction (v_cycle :611-624 and restrict_full_weighting
 // :397-424): coarse b = mean of the children's (b - sb - A x); x = in - s_in.
-template <typename T, typename B>
+// RX, RY, RZ are the refinement ratios (1 or 2); children summed in the
+// reference's dz, dy, dx order.
+template <typename T, typename B, int RX, int RY, int RZ>
 __global__ void __launch_bounds__(kTX* kTY)
     k_restrict_residual(OpInfo o, OpInfo oc, const B* __restrict__ b, const double* sb_ptr,
                         const T* __restrict__ in, const double* sin_ptr, T* __restrict__ bc,
-                        LevelScalars* lsc, int rx, int ry, int rz, int zm, int kchunk, RedBuf rb) {
+                        LevelScalars* lsc, int zm, int kchunk, RedBuf rb) {
   STENCIL_PROLOGUE(oc.L)
   using A = T;
   const double sb = *sb_ptr;
   const A sin = A(*sin_ptr);
-  const A inv_children = A(1.0 / double(rx * ry * rz));
+  const A inv_children = A(1.0 / double(RX * RY * RZ));
   double acc[1];
   zero(acc);
   if(valid) {
-    for(int kc = k0; kc < k1; ++kc) {
-      A sum = A(0);
-      for(int dz = 0; dz < rz; ++dz)
-        for(int dy = 0; dy < ry; ++dy)
-          for(int dx = 0; dx < rx; ++dx) {
-            const int fi = i * rx + dx, fj = j * ry + dy, fk = kc * rz + dz;
-            A c;
-            const A ax = apply_op<A>(o, fi, fj, fk,
-                                     [&](int ii, int jj, int kk) { return A(in[o.L.idx(ii, jj, kk)]) - sin; }, c);
-            sum += A(double(b[o.L.idx(fi, fj, fk)]) - sb) - ax;
-          }
-      const A v = inv_children * sum;
-      bc[oc.L.idx(i, j, kc)] = T(v);
-      acc[0] += double(v);
-    }
+    ColNb nb[RY][RX];
+#pragma unroll
+    for(int dy = 0; dy < RY; ++dy)
+#pragma unroll
+      for(int dx = 0; dx < RX; ++dx) nb[dy][dx] = col_nb(o, i * RX + dx, j * RY + dy);
+    auto val = [&](int ii, int jj, int kk) { return A(in[o.L.idx(ii, jj, kk)]) - sin; };
+    k_batched<2>(
+        k0, k1,
+        [&](int kc) {
+          A sum = A(0);
+#pragma unroll
+          for(int dz = 0; dz < RZ; ++dz)
+#pragma unroll
+            for(int dy = 0; dy < RY; ++dy)
+#pragma unroll
+              for(int dx = 0; dx < RX; ++dx) {
+                const int fi = i * RX + dx, fj = j * RY + dy, fk = kc * RZ + dz;
+                A c;
+                const A ax = apply_op<A>(o, nb[dy][dx], fi, fj, fk, val, c);
+                sum += A(double(b[o.L.idx(fi, fj, fk)]) - sb) - ax;
+              }
+          return inv_children * sum;
+        },
+        [&](int kc, A v) {
+          bc[oc.L.idx(i, j, kc)] = T(v);
+          acc[0] += double(v);
+        });
   }
   const bool mx[1] = {false};
   const int n = oc.L.count();
@@ -206,13 +283,13 @@ __global__ void __launch_bounds__(kTX* kTY)
 
 // Prolongation + first post-smoothing sweep (prolongate_and_add :426-451,
 // then smooth_jacobi): x3 = (in - s_in) + (e_parent - s_e); out = x3 +
-// omega (b - sb - A x3) / D.
+// omega (b - sb - A x3) / D.  SX, SY, SZ are log2 of the refinement ratios.
 template <typename T, typename B>
 __global__ void __launch_bounds__(kTX* kTY)
     k_prolong_smooth(OpInfo o, CLay Lc, const B* __restrict__ b, const double* sb_ptr,
                      const T* __restrict__ in, const double* sin_ptr, const T* __restrict__ ec,
-                     const double* sec_ptr, T* __restrict__ out, LevelScalars* ls, int rx, int ry,
-                     int rz, int zm, int kchunk, RedBuf rb) {
+                     const double* sec_ptr, T* __restrict__ out, LevelScalars* ls, int sx, int sy,
+                     int sz, int zm, int kchunk, RedBuf rb) {
   STENCIL_PROLOGUE(o.L)
   using A = T;
   const double sb = *sb_ptr;
@@ -221,24 +298,309 @@ __global__ void __launch_bounds__(kTX* kTY)
   double acc[1];
   zero(acc);
   if(valid) {
-    for(int k = k0; k < k1; ++k) {
-      const int q = o.L.idx(i, j, k);
-      A c;
-      const A ax = apply_op<A>(o, i, j, k,
-                               [&](int ii, int jj, int kk) {
-                                 return (A(in[o.L.idx(ii, jj, kk)]) - sin) +
-                                        (A(ec[Lc.idx(ii / rx, jj / ry, kk / rz)]) - sec);
-                               },
-                               c);
-      const A bq = A(double(b[q]) - sb);
-      const A v = c + A(kOmega) * (bq - ax) * A(inv_diag(o, i, j, k));
-      out[q] = T(v);
-      acc[0] += double(v);
-    }
+    const ColNb nb = col_nb(o, i, j);
+    const A om = A(kOmega);
+    auto val = [&](int ii, int jj, int kk) {
+      return (A(in[o.L.idx(ii, jj, kk)]) - sin) + (A(ec[Lc.idx(ii >> sx, jj >> sy, kk >> sz)]) - sec);
+    };
+    k_batched<kBatch>(
+        k0, k1,
+        [&](int k) {
+          A c;
+          const A ax = apply_op<A>(o, nb, i, j, k, val, c);
+          const A bq = A(double(b[o.L.idx(i, j, k)]) - sb);
+          return c + om * (bq - ax) * A(inv_diag(o, i, j, k));
+        },
+        [&](int k, A v) {
+          out[o.L.idx(i, j, k)] = T(v);
+          acc[0] += double(v);
+        });
   }
   const bool mx[1] = {false};
   const int n = o.L.count();
   reduce_finish<1>(acc, mx, rb, [=](const Sums<1>& s) { ls->sa = zm ? s.v[0] / n : 0.0; });
+}
+
+// ---------------------------------------------------------------------------
+// Row-vector kernels (vstencil.cuh) for levels whose rows split into 16-byte
+// vectors; the column kernels above serve the rest.
+// ---------------------------------------------------------------------------
+
+template <typename T>
+__host__ __device__ __forceinline__ bool vfits(const CLay& L) {
+  return vst::row_fits(L.nx, vst::Width<T>::W);
+}
+
+// Vector kernels can be switched off for comparisons: ORCHARD_B200_NO_VEC=1
+// (all) or a comma list of smooth, prolong, restrict, ap.  Read at each use so
+// that a process can compare both forms.
+bool vec_enabled(const char* which = "") {
+  const char* e = std::getenv("ORCHARD_B200_NO_VEC");
+  if(e == nullptr || e[0] == '\0' || e[0] == '0') return true;
+  if(e[0] == '1') return false;
+  return std::strstr(e, which) == nullptr || which[0] == '\0';
+}
+
+#define ROW_PROLOGUE(T)                                                          \
+  constexpr int W = vst::Width<T>::W;                                             \
+  const vst::RowGeom g = vst::row_geom<W>(o.L, o.periodic, o.dir_lo, o.dir_hi);   \
+  const int k0 = blockIdx.z * kchunk;                                             \
+  const int k1 = min(k0 + kchunk, o.L.nz);
+
+// Jacobi sweep (smooth_jacobi); same contract as k_smooth with which = 1.
+template <typename T, typename B>
+__global__ void __launch_bounds__(256)
+    k_vsmooth(OpInfo o, const B* __restrict__ b, const double* sb_ptr, const T* __restrict__ in,
+              const double* sin_ptr, T* __restrict__ out, LevelScalars* ls, int zm,
+              SolveScalars* sc, int kchunk, RedBuf rb) {
+  using A = T;
+  ROW_PROLOGUE(T)
+  using R = vst::Row<A, W>;
+  using RB = vst::Row<double, W>;
+  const double sb = *sb_ptr;
+  const A sin = A(*sin_ptr);
+  const A om = A(kOmega);
+  double acc[2] = {0.0, 0.0};
+  vst::march<A, W, RB>(
+      o, g, k0, k1,
+      [&](int i0, int jj, int kk) {
+        R r = vst::ld<A, W>(in + o.L.idx(i0, jj, kk));
+#pragma unroll
+        for(int t = 0; t < W; ++t) r.v[t] -= sin;
+        return r;
+      },
+      [&](int ii, int jj, int kk) { return A(in[o.L.idx(ii, jj, kk)]) - sin; },
+      [&](int i0, int jj, int kk) { return vst::ld<double, W>(b + o.L.idx(i0, jj, kk)); },
+      [&](int k, const R& c, const R& ax, const RB& bb) {
+        R v;
+        double bq[W];
+#pragma unroll
+        for(int t = 0; t < W; ++t) {
+          bq[t] = bb.v[t] - sb;
+          v.v[t] = c.v[t] + om * (A(bq[t]) - ax.v[t]) * A(inv_diag(o, g.i0 + t, g.j, k));
+        }
+        if(g.act) {
+          vst::st<T, W>(out + o.L.idx(g.i0, g.j, k), v);
+#pragma unroll
+          for(int t = 0; t < W; ++t) {
+            acc[0] += double(v.v[t]);
+            acc[1] += bq[t] * double(v.v[t]);
+          }
+        }
+      });
+  const bool mx[2] = {false, false};
+  const int n = o.L.count();
+  reduce_finish<2>(acc, mx, rb, [=](const Sums<2>& s) {
+    const double mean = zm ? s.v[0] / n : 0.0;
+    ls->sx = mean;
+    ls->sum_x = s.v[0];
+    if(sc != nullptr) {
+      // r.z with z = out - mean (linsolve/poisson_solver.cpp:749, :791)
+      const double rz_new = s.v[1] - mean * (sc->sum_r - sc->n * sc->sr);
+      if(sc->first) {
+        sc->rz = rz_new;
+      } else {
+        sc->beta = rz_new / sc->rz;
+        sc->rz = rz_new;
+      }
+    }
+  });
+}
+
+// Prolongation + first post-smoothing sweep; same contract as k_prolong_smooth.
+template <typename T, typename B>
+__global__ void __launch_bounds__(256)
+    k_vprolong_smooth(OpInfo o, CLay Lc, const B* __restrict__ b, const double* sb_ptr,
+                      const T* __restrict__ in, const double* sin_ptr, const T* __restrict__ ec,
+                      const double* sec_ptr, T* __restrict__ out, LevelScalars* ls, int sx, int sy,
+                      int sz, int zm, int kchunk, RedBuf rb) {
+  using A = T;
+  ROW_PROLOGUE(T)
+  using R = vst::Row<A, W>;
+  using RB = vst::Row<double, W>;
+  const double sb = *sb_ptr;
+  const A sin = A(*sin_ptr);
+  const A sec = A(*sec_ptr);
+  const A om = A(kOmega);
+  double acc[1] = {0.0};
+  vst::march<A, W, RB>(
+      o, g, k0, k1,
+      [&](int i0, int jj, int kk) {
+        R r = vst::ld<A, W>(in + o.L.idx(i0, jj, kk));
+        const int pj = jj >> sy, pk = kk >> sz;
+#pragma unroll
+        for(int t = 0; t < W; ++t) r.v[t] = (r.v[t] - sin) + (A(ec[Lc.idx((i0 + t) >> sx, pj, pk)]) - sec);
+        return r;
+      },
+      [&](int ii, int jj, int kk) {
+        return (A(in[o.L.idx(ii, jj, kk)]) - sin) + (A(ec[Lc.idx(ii >> sx, jj >> sy, kk >> sz)]) - sec);
+      },
+      [&](int i0, int jj, int kk) { return vst::ld<double, W>(b + o.L.idx(i0, jj, kk)); },
+      [&](int k, const R& c, const R& ax, const RB& bb) {
+        R v;
+#pragma unroll
+        for(int t = 0; t < W; ++t)
+          v.v[t] = c.v[t] + om * (A(bb.v[t] - sb) - ax.v[t]) * A(inv_diag(o, g.i0 + t, g.j, k));
+        if(g.act) {
+          vst::st<T, W>(out + o.L.idx(g.i0, g.j, k), v);
+#pragma unroll
+          for(int t = 0; t < W; ++t) acc[0] += double(v.v[t]);
+        }
+      });
+  const bool mx[1] = {false};
+  const int n = o.L.count();
+  reduce_finish<1>(acc, mx, rb, [=](const Sums<1>& s) { ls->sa = zm ? s.v[0] / n : 0.0; });
+}
+
+// A p; same contract as k_apply_ap.
+__global__ void __launch_bounds__(256)
+    k_vapply_ap(OpInfo o, const double* __restrict__ p, double* __restrict__ ap, SolveScalars* sc,
+                int kchunk, RedBuf rb) {
+  ROW_PROLOGUE(double)
+  using R = vst::Row<double, W>;
+  const double sp = sc->sp;
+  double acc[3] = {0.0, 0.0, 0.0};
+  vst::march<double, W, int>(
+      o, g, k0, k1,
+      [&](int i0, int jj, int kk) {
+        R r = vst::ld<double, W>(p + o.L.idx(i0, jj, kk));
+#pragma unroll
+        for(int t = 0; t < W; ++t) r.v[t] -= sp;
+        return r;
+      },
+      [&](int ii, int jj, int kk) { return p[o.L.idx(ii, jj, kk)] - sp; },
+      [&](int, int, int) { return 0; },
+      [&](int k, const R& c, const R& ax, int) {
+        if(g.act) {
+          vst::st<double, W>(ap + o.L.idx(g.i0, g.j, k), ax);
+#pragma unroll
+          for(int t = 0; t < W; ++t) {
+            acc[0] += ax.v[t];
+            acc[1] += c.v[t] * ax.v[t];
+            acc[2] += c.v[t];
+          }
+        }
+      });
+  const bool mx[3] = {false, false, false};
+  reduce_finish<3>(acc, mx, rb, [=](const Sums<3>& s) {
+    const double sap = sc->zero_mean ? s.v[0] / sc->n : 0.0;
+    sc->sap = sap;
+    const double pap = s.v[1] - sap * s.v[2];
+    sc->pap = pap;
+    if(fabs(pap) < kSmallNumber) {
+      sc->stop = 1;
+    } else {
+      sc->alpha = sc->rz / pap;
+    }
+  });
+}
+
+// Residual + 2x2x2 restriction on row vectors: a thread owns W fine cells of
+// the two fine rows of a coarse row (W/2 coarse cells) and marches coarse
+// planes (two fine planes each).
+template <typename T, typename B>
+__global__ void __launch_bounds__(256)
+    k_vrestrict(OpInfo o, OpInfo oc, const B* __restrict__ b, const double* sb_ptr,
+                const T* __restrict__ in, const double* sin_ptr, T* __restrict__ bc,
+                LevelScalars* lsc, int zm, int kchunk, RedBuf rb) {
+  using A = T;
+  constexpr int W = vst::Width<T>::W;
+  using R = vst::Row<A, W>;
+  const CLay& L = o.L;
+  const int lane = threadIdx.x;
+  int i0 = (blockIdx.x * 32 + lane) * W;
+  const int jc = blockIdx.y * 8 + threadIdx.y;
+  const bool act = i0 < L.nx && jc < oc.L.ny;
+  if(i0 >= L.nx) i0 = L.nx - W;
+  const int jcc = jc < oc.L.ny ? jc : oc.L.ny - 1;
+  const int kc0 = blockIdx.z * kchunk;
+  const int kc1 = min(kc0 + kchunk, oc.L.nz);
+  const double sb = *sb_ptr;
+  const A sin = A(*sin_ptr);
+  const A ix = A(o.inv2[0]), iy = A(o.inv2[1]), iz = A(o.inv2[2]);
+  const int jr[2] = {2 * jcc, 2 * jcc + 1};
+  int jdn, jup;
+  double sdn, sup;
+  nb_lo(jr[0], L.ny, o.periodic[1], o.dir_lo[1], jdn, sdn);
+  nb_hi(jr[1], L.ny, o.periodic[1], o.dir_hi[1], jup, sup);
+  const bool need_l = lane == 0 || i0 == 0;
+  const bool need_r = lane == 31 || i0 + W >= L.nx;
+  int xl, xr;
+  double sxl, sxr;
+  nb_lo(i0, L.nx, o.periodic[0], o.dir_lo[0], xl, sxl);
+  nb_hi(i0 + W - 1, L.nx, o.periodic[0], o.dir_hi[0], xr, sxr);
+  auto rowv = [&](int jj, int kk) {
+    R r = vst::ld<A, W>(in + L.idx(i0, jj, kk));
+#pragma unroll
+    for(int t = 0; t < W; ++t) r.v[t] -= sin;
+    return r;
+  };
+  auto zrowv = [&](int jj, int kk) {
+    double sg;
+    const int kz = vst::zrow(kk, L.nz, o.periodic[2], o.dir_lo[2], o.dir_hi[2], sg);
+    R r = rowv(jj, kz);
+#pragma unroll
+    for(int t = 0; t < W; ++t) r.v[t] *= A(sg);
+    return r;
+  };
+  double acc[1] = {0.0};
+  for(int kc = kc0; kc < kc1; ++kc) {
+    const int kf = 2 * kc;
+    // rows j0, j1 at planes kf-1 .. kf+2, neighbour rows at kf, kf+1
+    R q[2][4];
+#pragma unroll
+    for(int r = 0; r < 2; ++r)
+#pragma unroll
+      for(int z = 0; z < 4; ++z) q[r][z] = zrowv(jr[r], kf - 1 + z);
+    R dn[2], up[2];
+    A hl[2][2], hr[2][2];
+    vst::Row<double, W> bb[2][2];
+#pragma unroll
+    for(int z = 0; z < 2; ++z) {
+      dn[z] = rowv(jdn, kf + z);
+      up[z] = rowv(jup, kf + z);
+#pragma unroll
+      for(int t = 0; t < W; ++t) {
+        dn[z].v[t] *= A(sdn);
+        up[z].v[t] *= A(sup);
+      }
+#pragma unroll
+      for(int r = 0; r < 2; ++r) {
+        hl[r][z] = need_l ? A(sxl) * (A(in[L.idx(xl, jr[r], kf + z)]) - sin) : A(0);
+        hr[r][z] = need_r ? A(sxr) * (A(in[L.idx(xr, jr[r], kf + z)]) - sin) : A(0);
+        bb[r][z] = vst::ld<double, W>(b + L.idx(i0, jr[r], kf + z));
+      }
+    }
+    A csum[W / 2];
+#pragma unroll
+    for(int c = 0; c < W / 2; ++c) csum[c] = A(0);
+#pragma unroll
+    for(int z = 0; z < 2; ++z)
+#pragma unroll
+      for(int r = 0; r < 2; ++r) {
+        const R& cen = q[r][z + 1];
+        const A from_l = __shfl_up_sync(0xffffffffu, cen.v[W - 1], 1);
+        const A from_r = __shfl_down_sync(0xffffffffu, cen.v[0], 1);
+        const A left = need_l ? hl[r][z] : from_l;
+        const A right = need_r ? hr[r][z] : from_r;
+        const R& d = r == 0 ? dn[z] : q[0][z + 1];
+        const R& u = r == 0 ? q[1][z + 1] : up[z];
+        const R ax = vst::row_ax<A, W>(cen, left, right, d, u, q[r][z], q[r][z + 2], ix, iy, iz);
+#pragma unroll
+        for(int t = 0; t < W; ++t) csum[t / 2] += A(bb[r][z].v[t] - sb) - ax.v[t];
+      }
+    if(act) {
+#pragma unroll
+      for(int c = 0; c < W / 2; ++c) {
+        const A v = A(0.125) * csum[c];
+        bc[oc.L.idx(i0 / 2 + c, jc, kc)] = T(v);
+        acc[0] += double(v);
+      }
+    }
+  }
+  const bool mx[1] = {false};
+  const int n = oc.L.count();
+  reduce_finish<1>(acc, mx, rb, [=](const Sums<1>& s) { lsc->sb = zm ? s.v[0] / n : 0.0; });
 }
 
 // direct_coarse_solve (linsolve/poisson_solver.cpp:530-567) with the
@@ -247,7 +609,7 @@ __global__ void __launch_bounds__(kTX* kTY)
 template <typename T, typename B>
 __global__ void k_coarse_solve(int n, const int* __restrict__ swaps, const double* __restrict__ f,
                                const B* __restrict__ b, const double* sb_ptr, T* __restrict__ out,
-                               LevelScalars* ls, int zm, SolveScalars* sc, int first_rz) {
+                               LevelScalars* ls, int zm, SolveScalars* sc) {
   __shared__ double y[kMaxCoarse];
   __shared__ double red[32];
   const int t = threadIdx.x;
@@ -305,7 +667,7 @@ __global__ void k_coarse_solve(int n, const int* __restrict__ swaps, const doubl
     if(sc != nullptr) {
       double s = 0.0;
       for(int w = 0; w < (int(blockDim.x) + 31) / 32; ++w) s += red[w];
-      if(first_rz) {
+      if(sc->first) {
         sc->rz = s;
       } else {
         sc->beta = s / sc->rz;
@@ -322,22 +684,27 @@ __global__ void k_coarse_solve(int n, const int* __restrict__ swaps, const doubl
 // r = (b - sb) - A (x - sx); initial residual (linsolve/poisson_solver.cpp:717-739).
 __global__ void __launch_bounds__(kTX* kTY)
     k_initial_residual(OpInfo o, const double* __restrict__ b, const double* __restrict__ x,
-                       double* __restrict__ r, SolveScalars* sc, int kchunk, RedBuf rb) {
+                       double* __restrict__ r, SolveScalars* sc, int kchunk, RedBuf rb,
+                       cudaGraphConditionalHandle cond) {
   STENCIL_PROLOGUE(o.L)
   const double sb = sc->sb, sx = sc->sx;
   double acc[2];
   zero(acc);
   if(valid) {
-    for(int k = k0; k < k1; ++k) {
-      const int q = o.L.idx(i, j, k);
-      double c;
-      const double ax = apply_op<double>(o, i, j, k,
-                                         [&](int ii, int jj, int kk) { return x[o.L.idx(ii, jj, kk)] - sx; }, c);
-      const double v = (b[q] - sb) - ax;
-      r[q] = v;
-      acc[0] += v;
-      acc[1] += v * v;
-    }
+    const ColNb nb = col_nb(o, i, j);
+    auto val = [&](int ii, int jj, int kk) { return x[o.L.idx(ii, jj, kk)] - sx; };
+    k_batched<kBatch>(
+        k0, k1,
+        [&](int k) {
+          double c;
+          const double ax = apply_op<double>(o, nb, i, j, k, val, c);
+          return (b[o.L.idx(i, j, k)] - sb) - ax;
+        },
+        [&](int k, double v) {
+          r[o.L.idx(i, j, k)] = v;
+          acc[0] += v;
+          acc[1] += v * v;
+        });
   }
   const bool mx[2] = {false, false};
   reduce_finish<2>(acc, mx, rb, [=](const Sums<2>& s) {
@@ -354,6 +721,11 @@ __global__ void __launch_bounds__(kTX* kTY)
     sc->stop = 0;
     sc->converged = r0 <= sc->tol ? 1 : 0;
     if(sc->converged) sc->rel = 0.0;
+    sc->first = 1;
+    sc->body_runs = 0;
+    sc->cont = sc->converged ? 0 : 1;
+    if(sc->hist != nullptr && sc->hist_cap > 0) sc->hist[0] = r0;
+    if(cond) cudaGraphSetConditional(cond, sc->cont);
   });
 }
 
@@ -361,24 +733,30 @@ __global__ void __launch_bounds__(kTX* kTY)
 template <typename T>
 __global__ void __launch_bounds__(kTX* kTY)
     k_update_p(CLay L, const T* __restrict__ z, const LevelScalars* ls0, double* __restrict__ p,
-               SolveScalars* sc, int first, int kchunk, RedBuf rb) {
+               SolveScalars* sc, int kchunk, RedBuf rb) {
   STENCIL_PROLOGUE(L)
+  const int first = sc->first;
   const double sz = ls0->sx;
   const double beta = first ? 0.0 : sc->beta;
   const double sp = sc->sp;
   double acc[1];
   zero(acc);
   if(valid) {
-    for(int k = k0; k < k1; ++k) {
-      const int q = L.idx(i, j, k);
-      const double v = first ? double(z[q]) - sz : (double(z[q]) - sz) + beta * (p[q] - sp);
-      p[q] = v;
-      acc[0] += v;
-    }
+    k_batched<kBatch>(
+        k0, k1,
+        [&](int k) {
+          const int q = L.idx(i, j, k);
+          return first ? double(z[q]) - sz : (double(z[q]) - sz) + beta * (p[q] - sp);
+        },
+        [&](int k, double v) {
+          p[L.idx(i, j, k)] = v;
+          acc[0] += v;
+        });
   }
   const bool mx[1] = {false};
   reduce_finish<1>(acc, mx, rb, [=](const Sums<1>& s) {
     sc->sp = sc->zero_mean ? s.v[0] / sc->n : 0.0;
+    sc->first = 0;
   });
 }
 
@@ -391,16 +769,21 @@ __global__ void __launch_bounds__(kTX* kTY)
   double acc[3];
   zero(acc);
   if(valid) {
-    for(int k = k0; k < k1; ++k) {
-      const int q = o.L.idx(i, j, k);
-      double c;
-      const double v = apply_op<double>(o, i, j, k,
-                                        [&](int ii, int jj, int kk) { return p[o.L.idx(ii, jj, kk)] - sp; }, c);
-      ap[q] = v;
-      acc[0] += v;
-      acc[1] += c * v;
-      acc[2] += c;
-    }
+    const ColNb nb = col_nb(o, i, j);
+    auto val = [&](int ii, int jj, int kk) { return p[o.L.idx(ii, jj, kk)] - sp; };
+    k_batched<kBatch>(
+        k0, k1,
+        [&](int k) {
+          double c;
+          const double v = apply_op<double>(o, nb, i, j, k, val, c);
+          return Pair<double>{v, c};
+        },
+        [&](int k, Pair<double> r) {
+          ap[o.L.idx(i, j, k)] = r.v;
+          acc[0] += r.v;
+          acc[1] += r.w * r.v;
+          acc[2] += r.w;
+        });
   }
   const bool mx[3] = {false, false, false};
   reduce_finish<3>(acc, mx, rb, [=](const Sums<3>& s) {
@@ -421,27 +804,36 @@ __global__ void __launch_bounds__(kTX* kTY)
 __global__ void __launch_bounds__(kTX* kTY)
     k_update_xr(CLay L, double* __restrict__ x, double* __restrict__ r,
                 const double* __restrict__ p, const double* __restrict__ ap, SolveScalars* sc,
-                int kchunk, RedBuf rb) {
+                int kchunk, RedBuf rb, cudaGraphConditionalHandle cond) {
   STENCIL_PROLOGUE(L)
   const int stop = sc->stop;
   const double alpha = sc->alpha, sx = sc->sx, sr = sc->sr, sp = sc->sp, sap = sc->sap;
   double acc[3];
   zero(acc);
   if(valid && !stop) {
-    for(int k = k0; k < k1; ++k) {
-      const int q = L.idx(i, j, k);
-      const double xv = (x[q] - sx) + alpha * (p[q] - sp);
-      const double rv = (r[q] - sr) - alpha * (ap[q] - sap);
-      x[q] = xv;
-      r[q] = rv;
-      acc[0] += xv;
-      acc[1] += rv;
-      acc[2] += rv * rv;
-    }
+    k_batched<kBatch>(
+        k0, k1,
+        [&](int k) {
+          const int q = L.idx(i, j, k);
+          return Pair<double>{(x[q] - sx) + alpha * (p[q] - sp), (r[q] - sr) - alpha * (ap[q] - sap)};
+        },
+        [&](int k, Pair<double> v) {
+          const int q = L.idx(i, j, k);
+          x[q] = v.v;
+          r[q] = v.w;
+          acc[0] += v.v;
+          acc[1] += v.w;
+          acc[2] += v.w * v.w;
+        });
   }
   const bool mx[3] = {false, false, false};
   reduce_finish<3>(acc, mx, rb, [=](const Sums<3>& s) {
-    if(sc->stop) return;
+    sc->body_runs += 1;
+    if(sc->stop) {
+      sc->cont = 0;
+      if(cond) cudaGraphSetConditional(cond, 0);
+      return;
+    }
     const int n = sc->n;
     const int zm = sc->zero_mean;
     sc->sx = zm ? s.v[0] / n : 0.0;
@@ -453,6 +845,10 @@ __global__ void __launch_bounds__(kTX* kTY)
     sc->iterations += 1;
     sc->rel = sc->r0 > 0.0 ? sc->rnorm / sc->r0 : 0.0;
     if(sc->rel <= sc->tol) sc->converged = 1;
+    if(sc->hist != nullptr && sc->iterations < sc->hist_cap) sc->hist[sc->iterations] = sc->rnorm;
+    // the reference's loop: at most max_iterations iterations, stop on convergence
+    sc->cont = (sc->converged || sc->iterations >= sc->max_it) ? 0 : 1;
+    if(cond) cudaGraphSetConditional(cond, sc->cont);
   });
 }
 
@@ -495,7 +891,15 @@ struct PoissonPlan {
   double* factors = nullptr;
   LevelScalars* ls = nullptr;  // device, one per level
   double *b = nullptr, *x = nullptr, *r = nullptr, *p = nullptr, *ap = nullptr;
+  double* hist = nullptr;
+  int hist_cap = 0;
   size_t bytes = 0;
+  // the whole solve as one CUDA graph (built on first use)
+  bool use_graph = true;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  long long pre_counts[kKernelCount] = {};
+  long long body_counts[kKernelCount] = {};
 };
 
 namespace {
@@ -705,6 +1109,8 @@ PoissonPlan* poisson_plan_create(const Grid& g, const PBC& pbc_in, int precision
   OFB_CHECK(cudaMalloc(&P->ap, nf * sizeof(double)));
   OFB_CHECK(cudaMemset(P->p, 0, nf * sizeof(double)));
   P->bytes += 5 * nf * sizeof(double);
+  const char* no_graph = std::getenv("ORCHARD_B200_NO_GRAPH");
+  P->use_graph = !(no_graph != nullptr && no_graph[0] == '1');
   return P;
 }
 
@@ -716,6 +1122,9 @@ void poisson_plan_destroy(PoissonPlan* P) {
     cudaFree(lv.b);
     cudaFree(lv.invd);
   }
+  if(P->exec) cudaGraphExecDestroy(P->exec);
+  if(P->graph) cudaGraphDestroy(P->graph);
+  cudaFree(P->hist);
   cudaFree(P->ls);
   cudaFree(P->swaps);
   cudaFree(P->factors);
@@ -735,10 +1144,36 @@ double* poisson_x(PoissonPlan* P) { return P->x; }
 
 namespace {
 
+template <typename T, typename B, int RX, int RY, int RZ>
+void launch_restrict_r(const Level& lv, const Level& cv, const B* b, const double* sb_ptr,
+                       const T* x, const double* sx_ptr, T* bc, LevelScalars* lsc, int zm,
+                       const Launch3& lc, RedBuf rb, cudaStream_t s) {
+  k_restrict_residual<T, B, RX, RY, RZ><<<lc.grid, lc.block, 0, s>>>(lv.op, cv.op, b, sb_ptr, x,
+                                                                     sx_ptr, bc, lsc, zm,
+                                                                     lc.kchunk, rb);
+}
+
+template <typename T, typename B>
+void launch_restrict(const Level& lv, const Level& cv, const B* b, const double* sb_ptr, const T* x,
+                     const double* sx_ptr, T* bc, LevelScalars* lsc, int zm, const Launch3& lc,
+                     RedBuf rb, cudaStream_t s) {
+  const int code = (lv.rx == 2 ? 4 : 0) + (lv.ry == 2 ? 2 : 0) + (lv.rz == 2 ? 1 : 0);
+  switch(code) {
+    case 7: launch_restrict_r<T, B, 2, 2, 2>(lv, cv, b, sb_ptr, x, sx_ptr, bc, lsc, zm, lc, rb, s); break;
+    case 6: launch_restrict_r<T, B, 2, 2, 1>(lv, cv, b, sb_ptr, x, sx_ptr, bc, lsc, zm, lc, rb, s); break;
+    case 5: launch_restrict_r<T, B, 2, 1, 2>(lv, cv, b, sb_ptr, x, sx_ptr, bc, lsc, zm, lc, rb, s); break;
+    case 4: launch_restrict_r<T, B, 2, 1, 1>(lv, cv, b, sb_ptr, x, sx_ptr, bc, lsc, zm, lc, rb, s); break;
+    case 3: launch_restrict_r<T, B, 1, 2, 2>(lv, cv, b, sb_ptr, x, sx_ptr, bc, lsc, zm, lc, rb, s); break;
+    case 2: launch_restrict_r<T, B, 1, 2, 1>(lv, cv, b, sb_ptr, x, sx_ptr, bc, lsc, zm, lc, rb, s); break;
+    case 1: launch_restrict_r<T, B, 1, 1, 2>(lv, cv, b, sb_ptr, x, sx_ptr, bc, lsc, zm, lc, rb, s); break;
+    default: launch_restrict_r<T, B, 1, 1, 1>(lv, cv, b, sb_ptr, x, sx_ptr, bc, lsc, zm, lc, rb, s); break;
+  }
+}
+
 // v_cycle (linsolve/poisson_solver.cpp:597-633) from level l; the finest
 // level's rhs is the CG residual (double, shift sc->sr).
 template <typename T>
-void v_cycle(PoissonPlan* P, int l, SolveScalars* sc, int first_rz, RedBuf rb, cudaStream_t s) {
+void v_cycle(PoissonPlan* P, int l, SolveScalars* sc, RedBuf rb, cudaStream_t s) {
   Level& lv = P->levels[l];
   const int nl = static_cast<int>(P->levels.size());
   const int zm = P->zero_mean;
@@ -751,11 +1186,10 @@ void v_cycle(PoissonPlan* P, int l, SolveScalars* sc, int first_rz, RedBuf rb, c
     ProfScope ps(kKCoarseSolve, s);
     if(l == 0)
       k_coarse_solve<T, double><<<1, 256, 0, s>>>(P->coarse_n, P->swaps, P->factors, P->r, sb_ptr,
-                                                  x, ls, zm, rz_sc, first_rz);
+                                                  x, ls, zm, rz_sc);
     else
       k_coarse_solve<T, T><<<1, 256, 0, s>>>(P->coarse_n, P->swaps, P->factors,
-                                            static_cast<const T*>(lv.b), sb_ptr, x, ls, zm,
-                                            rz_sc, first_rz);
+                                            static_cast<const T*>(lv.b), sb_ptr, x, ls, zm, rz_sc);
     OFB_LAUNCH_CHECK("k_coarse_solve");
     return;
   }
@@ -770,29 +1204,53 @@ void v_cycle(PoissonPlan* P, int l, SolveScalars* sc, int first_rz, RedBuf rb, c
       ProfScope ps(fine ? kKSmoothFirstFine : kKCoarseLevels, s);
       k_smooth_first<T, B><<<ln.grid, ln.block, 0, s>>>(lv.op, bptr, sb_ptr, a, ls, zm, ln.kchunk, rb);
     }
+    const bool vec = vfits<T>(lv.L) && vec_enabled();
+    const bool vsm = vec && vec_enabled("smooth");
+    const bool vpr = vec && vec_enabled("prolong");
+    const bool vre = vec && vec_enabled("restrict");
+    const vst::RowLaunch lr = vst::row_launch(lv.L.nx, lv.L.ny, lv.L.nz, vst::Width<T>::W, 16);
     {
       ProfScope ps(fine ? kKSmoothFine : kKCoarseLevels, s);
-      k_smooth<T, B><<<ln.grid, ln.block, 0, s>>>(lv.op, bptr, sb_ptr, a, &ls->sa, x, ls, 1, zm,
-                                                  nullptr, 0, ln.kchunk, rb);
+      if(vsm)
+        k_vsmooth<T, B><<<lr.grid, lr.block, 0, s>>>(lv.op, bptr, sb_ptr, a, &ls->sa, x, ls, zm,
+                                                     nullptr, lr.kchunk, rb);
+      else
+        k_smooth<T, B><<<ln.grid, ln.block, 0, s>>>(lv.op, bptr, sb_ptr, a, &ls->sa, x, ls, 1, zm,
+                                                    nullptr, ln.kchunk, rb);
     }
     {
       ProfScope ps(fine ? kKRestrictFine : kKCoarseLevels, s);
-      k_restrict_residual<T, B><<<lc.grid, lc.block, 0, s>>>(lv.op, cv.op, bptr, sb_ptr, x, &ls->sx,
-                                                           static_cast<T*>(cv.b), lsc, lv.rx,
-                                                           lv.ry, lv.rz, zm, lc.kchunk, rb);
+      if(vre && lv.rx == 2 && lv.ry == 2 && lv.rz == 2) {
+        const vst::RowLaunch lrc =
+            vst::row_launch(lv.L.nx, cv.L.ny, cv.L.nz, vst::Width<T>::W, 8);
+        k_vrestrict<T, B><<<lrc.grid, lrc.block, 0, s>>>(lv.op, cv.op, bptr, sb_ptr, x, &ls->sx,
+                                                         static_cast<T*>(cv.b), lsc, zm,
+                                                         lrc.kchunk, rb);
+      } else
+        launch_restrict<T, B>(lv, cv, bptr, sb_ptr, x, &ls->sx, static_cast<T*>(cv.b), lsc, zm,
+                              lc, rb, s);
     }
     OFB_LAUNCH_CHECK("v_cycle descent");
-    v_cycle<T>(P, l + 1, sc, first_rz, rb, s);
+    v_cycle<T>(P, l + 1, sc, rb, s);
     {
       ProfScope ps(fine ? kKProlongFine : kKCoarseLevels, s);
-      k_prolong_smooth<T, B><<<ln.grid, ln.block, 0, s>>>(lv.op, cv.L, bptr, sb_ptr, x, &ls->sx,
-                                                          static_cast<const T*>(cv.x), &lsc->sx, a,
-                                                          ls, lv.rx, lv.ry, lv.rz, zm, ln.kchunk, rb);
+      if(vpr)
+        k_vprolong_smooth<T, B><<<lr.grid, lr.block, 0, s>>>(
+            lv.op, cv.L, bptr, sb_ptr, x, &ls->sx, static_cast<const T*>(cv.x), &lsc->sx, a, ls,
+            lv.rx == 2 ? 1 : 0, lv.ry == 2 ? 1 : 0, lv.rz == 2 ? 1 : 0, zm, lr.kchunk, rb);
+      else
+        k_prolong_smooth<T, B><<<ln.grid, ln.block, 0, s>>>(
+            lv.op, cv.L, bptr, sb_ptr, x, &ls->sx, static_cast<const T*>(cv.x), &lsc->sx, a, ls,
+            lv.rx == 2 ? 1 : 0, lv.ry == 2 ? 1 : 0, lv.rz == 2 ? 1 : 0, zm, ln.kchunk, rb);
     }
     {
       ProfScope ps(fine ? kKSmoothFine : kKCoarseLevels, s);
-      k_smooth<T, B><<<ln.grid, ln.block, 0, s>>>(lv.op, bptr, sb_ptr, a, &ls->sa, x, ls, 1, zm,
-                                                  rz_sc, first_rz, ln.kchunk, rb);
+      if(vsm)
+        k_vsmooth<T, B><<<lr.grid, lr.block, 0, s>>>(lv.op, bptr, sb_ptr, a, &ls->sa, x, ls, zm,
+                                                     rz_sc, lr.kchunk, rb);
+      else
+        k_smooth<T, B><<<ln.grid, ln.block, 0, s>>>(lv.op, bptr, sb_ptr, a, &ls->sa, x, ls, 1, zm,
+                                                    rz_sc, ln.kchunk, rb);
     }
     OFB_LAUNCH_CHECK("v_cycle ascent");
   };
@@ -800,67 +1258,137 @@ void v_cycle(PoissonPlan* P, int l, SolveScalars* sc, int first_rz, RedBuf rb, c
   else smooth_chain(static_cast<const T*>(lv.b));
 }
 
+// Initial residual and convergence test (linsolve/poisson_solver.cpp:717-739).
+void enqueue_pre(PoissonPlan* P, SolveScalars* sc, RedBuf rb, cudaStream_t s,
+                 cudaGraphConditionalHandle cond) {
+  const Level& l0 = P->levels[0];
+  const Launch3 ln = launch3(l0.L.nx, l0.L.ny, l0.L.nz);
+  ProfScope ps(kKInitResidual, s);
+  k_initial_residual<<<ln.grid, ln.block, 0, s>>>(l0.op, P->b, P->x, P->r, sc, ln.kchunk, rb, cond);
+  OFB_LAUNCH_CHECK("k_initial_residual");
+}
+
+// One body of the rotated PCG loop: z = M r, p = z + beta p, A p, x/r update
+// and the convergence test -- the reference's iteration (:750-806) with the
+// preconditioner moved to the top; the body count is the reference's
+// iteration count, and the first body forms p = z as the reference does
+// before its loop (:741-749).
+template <typename T>
+void enqueue_body(PoissonPlan* P, SolveScalars* sc, RedBuf rb, cudaStream_t s,
+                  cudaGraphConditionalHandle cond) {
+  const Level& l0 = P->levels[0];
+  const Launch3 ln = launch3(l0.L.nx, l0.L.ny, l0.L.nz);
+  v_cycle<T>(P, 0, sc, rb, s);
+  {
+    ProfScope ps(kKUpdateP, s);
+    k_update_p<T><<<ln.grid, ln.block, 0, s>>>(l0.L, static_cast<const T*>(l0.x), P->ls, P->p, sc,
+                                               ln.kchunk, rb);
+  }
+  {
+    ProfScope ps(kKApplyAp, s);
+    if(vfits<double>(l0.L) && vec_enabled() && vec_enabled("ap")) {
+      const vst::RowLaunch lr = vst::row_launch(l0.L.nx, l0.L.ny, l0.L.nz, 2, 16);
+      k_vapply_ap<<<lr.grid, lr.block, 0, s>>>(l0.op, P->p, P->ap, sc, lr.kchunk, rb);
+    }
+    else
+      k_apply_ap<<<ln.grid, ln.block, 0, s>>>(l0.op, P->p, P->ap, sc, ln.kchunk, rb);
+  }
+  {
+    ProfScope ps(kKUpdateXr, s);
+    k_update_xr<<<ln.grid, ln.block, 0, s>>>(l0.L, P->x, P->r, P->p, P->ap, sc, ln.kchunk, rb, cond);
+  }
+  OFB_LAUNCH_CHECK("pcg body");
+}
+
+// The whole solve as one graph: pre -> WHILE(cont) { body }.  The loop is
+// bounded by max_iterations (the body clears the condition), so the graph
+// always terminates.
+template <typename T>
+void build_graph(PoissonPlan* P, SolveScalars* sc, RedBuf rb, cudaStream_t s) {
+  cudaGraph_t g = nullptr;
+  OFB_CHECK(cudaGraphCreate(&g, 0));
+  cudaGraphConditionalHandle cond = 0;
+  OFB_CHECK(cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault));
+  for(int i = 0; i < kKernelCount; ++i) P->pre_counts[i] = P->body_counts[i] = 0;
+  prof_capture_begin(P->pre_counts);
+  OFB_CHECK(cudaStreamBeginCaptureToGraph(s, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  enqueue_pre(P, sc, rb, s, cond);
+  cudaStreamCaptureStatus status;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t ndeps = 0;
+  OFB_CHECK(cudaStreamGetCaptureInfo(s, &status, nullptr, nullptr, &deps, &ndeps));
+  std::vector<cudaGraphNode_t> leaf(deps, deps + ndeps);
+  OFB_CHECK(cudaStreamEndCapture(s, &g));
+  prof_capture_end();
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = cond;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t wnode;
+  OFB_CHECK(cudaGraphAddNode(&wnode, g, leaf.data(), leaf.size(), &cp));
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  prof_capture_begin(P->body_counts);
+  OFB_CHECK(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeThreadLocal));
+  enqueue_body<T>(P, sc, rb, s, cond);
+  OFB_CHECK(cudaStreamEndCapture(s, &body));
+  prof_capture_end();
+  OFB_CHECK(cudaGraphInstantiate(&P->exec, g, 0));
+  P->graph = g;
+}
+
 template <typename T>
 void solve_impl(PoissonPlan* P, int max_iterations, double tolerance, SolveScalars* sc,
                 SolveScalars* host, RedBuf rb, cudaStream_t s, double* history, int history_cap) {
   const Level& l0 = P->levels[0];
-  const Launch3 ln = launch3(l0.L.nx, l0.L.ny, l0.L.nz);
+  if(P->hist_cap < max_iterations + 1) {
+    if(P->hist) cudaFree(P->hist);
+    P->hist = nullptr;
+    OFB_CHECK(cudaMalloc(&P->hist, sizeof(double) * (max_iterations + 1)));
+    P->hist_cap = max_iterations + 1;
+  }
   // sc->sb and sc->sx were set by the kernels that filled b and x.
-  SolveScalars init{};
   OFB_CHECK(cudaMemcpyAsync(host, sc, sizeof(SolveScalars), cudaMemcpyDeviceToHost, s));
   OFB_CHECK(cudaStreamSynchronize(s));
-  init = *host;
+  SolveScalars init = *host;
   init.zero_mean = P->zero_mean;
   init.n = l0.L.count();
   init.tol = tolerance;
+  init.max_it = max_iterations;
+  init.hist = P->hist;
+  init.hist_cap = P->hist_cap;
   if(!P->zero_mean) {
     init.sb = 0.0;
     init.sx = 0.0;
     init.removed_rhs_mean = 0.0;
   }
   init.sp = 0.0;
-  OFB_CHECK(cudaMemcpyAsync(sc, &init, sizeof(SolveScalars), cudaMemcpyHostToDevice, s));
-  {
-    ProfScope ps(kKInitResidual, s);
-    k_initial_residual<<<ln.grid, ln.block, 0, s>>>(l0.op, P->b, P->x, P->r, sc, ln.kchunk, rb);
-  }
-  OFB_LAUNCH_CHECK("k_initial_residual");
-  OFB_CHECK(cudaMemcpyAsync(host, sc, sizeof(SolveScalars), cudaMemcpyDeviceToHost, s));
-  OFB_CHECK(cudaStreamSynchronize(s));
-  int nh = 0;
-  if(history && nh < history_cap) history[nh] = host->r0;
-  ++nh;
-  if(host->converged) return;
-  v_cycle<T>(P, 0, sc, 1, rb, s);
-  {
-    ProfScope ps(kKUpdateP, s);
-    k_update_p<T><<<ln.grid, ln.block, 0, s>>>(l0.L, static_cast<const T*>(l0.x), P->ls, P->p, sc, 1,
-                                               ln.kchunk, rb);
-  }
-  OFB_LAUNCH_CHECK("k_update_p");
-  for(int it = 0; it < max_iterations; ++it) {
-    {
-      ProfScope ps(kKApplyAp, s);
-      k_apply_ap<<<ln.grid, ln.block, 0, s>>>(l0.op, P->p, P->ap, sc, ln.kchunk, rb);
-    }
-    {
-      ProfScope ps(kKUpdateXr, s);
-      k_update_xr<<<ln.grid, ln.block, 0, s>>>(l0.L, P->x, P->r, P->p, P->ap, sc, ln.kchunk, rb);
-    }
-    OFB_LAUNCH_CHECK("k_update_xr");
+  *host = init;
+  OFB_CHECK(cudaMemcpyAsync(sc, host, sizeof(SolveScalars), cudaMemcpyHostToDevice, s));
+  const bool use_graph = P->use_graph && !prof_enabled();
+  if(use_graph) {
+    if(P->exec == nullptr) build_graph<T>(P, sc, rb, s);
+    OFB_CHECK(cudaGraphLaunch(P->exec, s));
     OFB_CHECK(cudaMemcpyAsync(host, sc, sizeof(SolveScalars), cudaMemcpyDeviceToHost, s));
     OFB_CHECK(cudaStreamSynchronize(s));
-    if(host->stop) break;
-    if(history && nh < history_cap) history[nh] = host->rnorm;
-    ++nh;
-    if(host->converged) break;
-    v_cycle<T>(P, 0, sc, 0, rb, s);
-    {
-      ProfScope ps(kKUpdateP, s);
-      k_update_p<T><<<ln.grid, ln.block, 0, s>>>(l0.L, static_cast<const T*>(l0.x), P->ls, P->p, sc,
-                                                 0, ln.kchunk, rb);
+    prof_add_counts(P->pre_counts, 1);
+    prof_add_counts(P->body_counts, host->body_runs);
+  } else {
+    enqueue_pre(P, sc, rb, s, 0);
+    OFB_CHECK(cudaMemcpyAsync(host, sc, sizeof(SolveScalars), cudaMemcpyDeviceToHost, s));
+    OFB_CHECK(cudaStreamSynchronize(s));
+    prof_collect();
+    while(host->cont) {
+      enqueue_body<T>(P, sc, rb, s, 0);
+      OFB_CHECK(cudaMemcpyAsync(host, sc, sizeof(SolveScalars), cudaMemcpyDeviceToHost, s));
+      OFB_CHECK(cudaStreamSynchronize(s));
+      prof_collect();
     }
-    OFB_LAUNCH_CHECK("k_update_p");
+  }
+  if(history != nullptr && history_cap > 0) {
+    const int n = std::min(history_cap, std::min(host->iterations + 1, P->hist_cap));
+    OFB_CHECK(cudaMemcpy(history, P->hist, sizeof(double) * n, cudaMemcpyDeviceToHost));
   }
 }
 
@@ -873,8 +1401,6 @@ void poisson_solve(PoissonPlan* P, int max_iterations, double tolerance, SolveSc
     solve_impl<float>(P, max_iterations, tolerance, sc_dev, sc_host, rb, s, history, history_cap);
   else
     solve_impl<double>(P, max_iterations, tolerance, sc_dev, sc_host, rb, s, history, history_cap);
-  OFB_CHECK(cudaMemcpyAsync(sc_host, sc_dev, sizeof(SolveScalars), cudaMemcpyDeviceToHost, s));
-  OFB_CHECK(cudaStreamSynchronize(s));
 }
 
 void launch_compact_to_pressure(const Grid& g, const double* x, const SolveScalars* sc,

@@ -28,6 +28,7 @@ struct Profiler {
   std::vector<Pending> pending;
   std::vector<cudaEvent_t> pool;
   cudaEvent_t cur_start[kKernelCount] = {};
+  long long* capture = nullptr;
 };
 
 Profiler& prof() {
@@ -58,6 +59,10 @@ const char* kNames[kKernelCount] = {
 void prof_launch(int id, cudaStream_t s, bool begin, int count) {
   Profiler& p = prof();
   std::lock_guard<std::mutex> lock(p.mu);
+  if(p.capture != nullptr) {
+    if(begin) p.capture[id] += count;
+    return;
+  }
   if(begin) {
     p.launches[id] += count;
     if(!p.enabled) return;
@@ -71,6 +76,30 @@ void prof_launch(int id, cudaStream_t s, bool begin, int count) {
   cudaEventRecord(e, s);
   p.pending.push_back(Pending{id, p.cur_start[id], e});
   p.cur_start[id] = nullptr;
+}
+
+bool prof_enabled() {
+  Profiler& p = prof();
+  std::lock_guard<std::mutex> lock(p.mu);
+  return p.enabled;
+}
+
+void prof_capture_begin(long long* counts) {
+  Profiler& p = prof();
+  std::lock_guard<std::mutex> lock(p.mu);
+  p.capture = counts;
+}
+
+void prof_capture_end() {
+  Profiler& p = prof();
+  std::lock_guard<std::mutex> lock(p.mu);
+  p.capture = nullptr;
+}
+
+void prof_add_counts(const long long* counts, long long times) {
+  Profiler& p = prof();
+  std::lock_guard<std::mutex> lock(p.mu);
+  for(int i = 0; i < kKernelCount; ++i) p.launches[i] += counts[i] * times;
 }
 
 void prof_collect() {

@@ -29,6 +29,12 @@ enum KernelClass : int {
 
 void prof_launch(int id, cudaStream_t s, bool begin, int count = 1);
 void prof_collect();
+bool prof_enabled();
+// While a graph is captured, launches are counted into `counts` (no events);
+// prof_add_counts later credits the replays.
+void prof_capture_begin(long long* counts);
+void prof_capture_end();
+void prof_add_counts(const long long* counts, long long times);
 
 // Brackets `count` kernel launches of one class: counts them and, when timing
 // is on, records an event pair around them on their stream.
