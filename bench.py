@@ -59,7 +59,8 @@ def bytes_per_launch(n, precision):
     d = 8
     t = 4 if precision == "mixed" else 8  # V-cycle level vectors
     return {
-        "predictor_rhs": 13 * d * N / 3,  # per component launch (7 reads, 6 writes over 3)
+        "predictor_rhs": 5 * d * N,  # per component: read f, p, prev, adv; write rhs
+        "advection": 4 * d * N,      # per component: read u, v, w; write adv
         "adi_sweep": 2 * d * N,
         "divergence_rhs": 5 * d * N,
         "pcg_initial_residual": 3 * d * N,

@@ -29,6 +29,12 @@ struct AdiAxis {
   double uc_over_gamma = 0.0;
   double inv_den = 0.0;
   size_t off = 0;           // offset of cu/ip/z in the coefficient buffer
+  // partition (SPIKE) solver, used when n is a multiple of 32 and >= 64:
+  // per-lane segment factors, spikes and the interface operator, all laid
+  // out [element][lane] so that a warp reads them with one coalesced load
+  bool partition = false;
+  int seg = 0;              // K = n / 32
+  size_t poff = 0;          // offset: cu[K][32], ip[K][32], v[K][32], w[K][32], gl[64][32], gr[64][32]
 };
 
 struct AdiPlan {
@@ -173,6 +179,60 @@ AdiPlan* adi_plan_create(const Grid& g, const VBC& bc, double alpha) {
       host.insert(host.end(), cu.begin(), cu.end());
       host.insert(host.end(), ip.begin(), ip.end());
       host.insert(host.end(), z.begin(), z.end());
+      if(n % 32 == 0 && n >= 64 && n / 32 <= 16) {
+        // Warp-scan form of the two Thomas recurrences (lane p owns the
+        // unknowns q = pK + j, j < K):
+        //   forward  m_q = ip_q r_q + f_q m_{q-1},  f_q = -lower ip_q
+        //   backward x_q = m_q + g_q x_{q+1},       g_q = -cu_q
+        // Lane-local products of f (resp. g) and the per-step multipliers of
+        // the Kogge-Stone scans are line-independent and stored here.
+        const int P = 32, K = n / 32;
+        std::vector<double> fB(K * P), gD(K * P), ipj(K * P), cuj(K * P), zj(K * P);
+        std::vector<double> mf(5 * P, 0.0), mb(5 * P, 0.0);
+        std::vector<double> lane_f(P), lane_g(P);
+        for(int lane = 0; lane < P; ++lane) {
+          double prod = 1.0;
+          for(int j = 0; j < K; ++j) {
+            const int q = lane * K + j;
+            const double f = q == 0 ? 0.0 : -(-beta) * ip[q];
+            prod = j == 0 ? f : prod * f;
+            fB[j * P + lane] = prod;
+            ipj[j * P + lane] = ip[q];
+            cuj[j * P + lane] = cu[q];
+            zj[j * P + lane] = z[q];
+          }
+          lane_f[lane] = prod;  // m_end = A + prod * m_in
+          double dprod = 1.0;
+          for(int j = K - 1; j >= 0; --j) {
+            const int q = lane * K + j;
+            const double g = -cu[q];
+            dprod = j == K - 1 ? g : dprod * g;
+            gD[j * P + lane] = dprod;
+          }
+          lane_g[lane] = dprod;  // x_first = C + dprod * x_in
+        }
+        // Kogge-Stone multipliers: inclusive scan of (a, b) maps; step s
+        // combines lane p with lane p - 2^s (forward) / p + 2^s (backward)
+        std::vector<double> cf = lane_f, cb = lane_g;
+        for(int st = 0; st < 5; ++st) {
+          const int d = 1 << st;
+          std::vector<double> nf = cf, nb = cb;
+          for(int lane = 0; lane < P; ++lane) {
+            mf[st * P + lane] = lane >= d ? cf[lane] : 0.0;
+            if(lane >= d) nf[lane] = cf[lane] * cf[lane - d];
+            mb[st * P + lane] = lane + d < P ? cb[lane] : 0.0;
+            if(lane + d < P) nb[lane] = cb[lane] * cb[lane + d];
+          }
+          cf = nf;
+          cb = nb;
+        }
+        A.partition = true;
+        A.seg = K;
+        A.poff = host.size();
+        for(auto* v : {&ipj, &fB, &cuj, &gD, &zj}) host.insert(host.end(), v->begin(), v->end());
+        host.insert(host.end(), mf.begin(), mf.end());
+        host.insert(host.end(), mb.begin(), mb.end());
+      }
     }
   }
   if(!host.empty()) {
@@ -249,6 +309,267 @@ __global__ void __launch_bounds__(128) k_adi_sweep(SweepArgs a, const double* __
   if(a.copy_duplicate) out[base + a.dup_index * st] = dst[0];
 }
 
+// Shared-memory line solver: one warp stages `lines` whole lines in shared
+// memory (coalesced: x-lines load row segments, y/z-lines load 32 adjacent
+// i-lines so each warp load is one contiguous row), solves them there with
+// the shared Thomas factors and the Sherman-Morrison update, and stores them
+// back coalesced.  Lines of an x-sweep are stored [line][n + 1] (the pad
+// spreads a warp's column accesses over the banks), lines of a y/z sweep
+// [n][lines] (a warp reads one row).
+template <bool XLINES>
+__global__ void __launch_bounds__(32) k_adi_tile(SweepArgs a, const double* __restrict__ in,
+                                                 double* __restrict__ out, int lines) {
+  extern __shared__ double tile[];
+  const Lay& L = a.L;
+  const int axis = a.axis;
+  const int a1 = axis == 0 ? 1 : 0;
+  const int a2 = axis == 2 ? 1 : 2;
+  const int n = a.n;
+  const int st = L.stride(axis);
+  const int t = threadIdx.x;
+  const int n1 = L.n(a1);
+  const int n2 = L.n(a2);
+  // line l of this block -> storage base of its position 0 along the axis
+  auto line_base = [&](int l, bool& ok) {
+    int c1, c2;
+    if(XLINES) {
+      const int flat = blockIdx.x * lines + l;
+      c1 = flat % n1;
+      c2 = flat / n1;
+      ok = c2 < n2;
+    } else {
+      c1 = blockIdx.x * lines + l;
+      c2 = blockIdx.y;
+      ok = c1 < n1;
+    }
+    if(!ok) {
+      c1 = 0;
+      c2 = 0;
+    }
+    int c[3] = {0, 0, 0};
+    c[a1] = c1 + 1;
+    c[a2] = c2 + 1;
+    return L.idx(c[0], c[1], c[2]) + a.begin * st;
+  };
+  auto at = [&](int l, int q) -> double& {
+    return XLINES ? tile[l * (n + 1) + q] : tile[q * lines + l];
+  };
+  // load
+  if(XLINES) {
+    for(int l = 0; l < lines; ++l) {
+      bool ok;
+      const int base = line_base(l, ok);
+      if(!ok) continue;
+      for(int q = t; q < n; q += 32) at(l, q) = in[base + q];
+    }
+  } else {
+    for(int q = 0; q < n; ++q) {
+      for(int l = t; l < lines; l += 32) {
+        bool ok;
+        const int base = line_base(l, ok);
+        if(ok) at(l, q) = in[base + q * st];
+      }
+    }
+  }
+  __syncwarp();
+  // solve line t
+  if(t < lines) {
+    double r = at(t, 0) + a.rhs_first;
+    if(n == 1) r += a.rhs_last;
+    double m = r * __ldg(&a.ip[0]);
+    at(t, 0) = m;
+    for(int q = 1; q < n; ++q) {
+      double rq = at(t, q);
+      if(q == n - 1) rq += a.rhs_last;
+      m = (rq - a.lower * m) * __ldg(&a.ip[q]);
+      at(t, q) = m;
+    }
+    const double x_last = m;
+    double x = m;
+    for(int q = n - 2; q >= 0; --q) {
+      x = at(t, q) - __ldg(&a.cu[q]) * x;
+      at(t, q) = x;
+    }
+    if(a.periodic && n > 1) {
+      const double factor = (x + a.uc_over_gamma * x_last) * a.inv_den;
+      for(int q = 0; q < n; ++q) at(t, q) -= factor * __ldg(&a.z[q]);
+    }
+  }
+  __syncwarp();
+  // store (and the duplicated periodic face)
+  if(XLINES) {
+    for(int l = 0; l < lines; ++l) {
+      bool ok;
+      const int base = line_base(l, ok);
+      if(!ok) continue;
+      for(int q = t; q < n; q += 32) out[base + q] = at(l, q);
+      if(a.copy_duplicate && t == 0) out[base - a.begin * st + a.dup_index * st] = at(l, 0);
+    }
+  } else {
+    for(int q = 0; q < n; ++q) {
+      for(int l = t; l < lines; l += 32) {
+        bool ok;
+        const int base = line_base(l, ok);
+        if(ok) out[base + q * st] = at(l, q);
+      }
+    }
+    if(a.copy_duplicate) {
+      for(int l = t; l < lines; l += 32) {
+        bool ok;
+        const int base = line_base(l, ok);
+        if(ok) out[base - a.begin * st + a.dup_index * st] = at(l, 0);
+      }
+    }
+  }
+}
+
+constexpr size_t kAdiTileBytes = 64 * 1024;
+
+struct ScanArgs {
+  const double* ip;  // [K][32]
+  const double* fB;  // lane-local forward products
+  const double* cu;
+  const double* gD;  // lane-local backward products
+  const double* z;   // Sherman-Morrison vector
+  const double* mf;  // [5][32] forward scan multipliers
+  const double* mb;  // [5][32] backward scan multipliers
+  int K;
+};
+
+// Warp-scan line solver: a block of 16 warps stages 16 lines in shared
+// memory (element q = pK + j of a line at [j][p], so a warp's accesses are
+// conflict-free); warp w solves line w.  Lane p evaluates its K forward
+// elimination steps as an affine map of the unknown carried in from lane p-1,
+// the 32 maps are composed by a Kogge-Stone scan over shuffles, and the same
+// is done for back substitution; the periodic Sherman-Morrison update
+// (solver/projection.cpp:607-616) follows.  Same Thomas factors as the
+// reference's recurrences; the association of the products differs, so
+// results agree to rounding.
+template <bool XLINES>
+__global__ void __launch_bounds__(512) k_adi_scan(SweepArgs a, ScanArgs sa,
+                                                  const double* __restrict__ in,
+                                                  double* __restrict__ out) {
+  constexpr int LB = 16;
+  extern __shared__ double tile[];
+  const Lay& L = a.L;
+  const int axis = a.axis;
+  const int a1 = axis == 0 ? 1 : 0;
+  const int a2 = axis == 2 ? 1 : 2;
+  const int n = a.n;
+  const int K = sa.K;
+  const int S = n + 1;  // per-line stride in the tile
+  const int st = L.stride(axis);
+  const int n1 = L.n(a1), n2 = L.n(a2);
+  const int tid = threadIdx.x + 32 * threadIdx.y;
+  const int lane = threadIdx.x, wl = threadIdx.y;
+  auto line_base = [&](int l, bool& ok) {
+    int c1, c2;
+    if(XLINES) {
+      const int flat = blockIdx.x * LB + l;
+      c1 = flat % n1;
+      c2 = flat / n1;
+      ok = c2 < n2;
+    } else {
+      c1 = blockIdx.x * LB + l;
+      c2 = blockIdx.y;
+      ok = c1 < n1;
+    }
+    if(!ok) c1 = c2 = 0;
+    int c[3] = {0, 0, 0};
+    c[a1] = c1 + 1;
+    c[a2] = c2 + 1;
+    return L.idx(c[0], c[1], c[2]) + a.begin * st;
+  };
+  auto slot = [&](int l, int q) { return l * S + (q % K) * 32 + q / K; };
+  if(XLINES) {
+    bool ok;
+    const int base = line_base(wl, ok);
+    if(ok)
+      for(int q = lane; q < n; q += 32) tile[slot(wl, q)] = in[base + q];
+  } else {
+    const int l = tid % LB;
+    bool ok;
+    const int base = line_base(l, ok);
+    if(ok)
+      for(int q = tid / LB; q < n; q += 512 / LB) tile[slot(l, q)] = in[base + q * st];
+  }
+  __syncthreads();
+  {
+    double* line = tile + wl * S;
+    // forward elimination, lane-local part: m_{pK+j} = A_j + fB_j m_in
+    double acc = 0.0;
+    for(int j = 0; j < K; ++j) {
+      const int q = lane * K + j;
+      double r = line[j * 32 + lane];
+      if(q == 0) r += a.rhs_first;
+      if(q == n - 1) r += a.rhs_last;
+      const double ipq = __ldg(&sa.ip[j * 32 + lane]);
+      // f_q = lower_coupling * ip_q with the coupling -(-beta) folded in
+      const double f = q == 0 ? 0.0 : -a.lower * ipq;
+      acc = j == 0 ? r * ipq : r * ipq + f * acc;
+      line[j * 32 + lane] = acc;  // A_j
+    }
+    // inclusive scan of lane maps: val = m at the lane's last unknown
+    double val = acc;
+#pragma unroll
+    for(int s = 0; s < 5; ++s) {
+      const double up = __shfl_up_sync(0xffffffffu, val, 1 << s);
+      val += __ldg(&sa.mf[s * 32 + lane]) * up;
+    }
+    double m_in = __shfl_up_sync(0xffffffffu, val, 1);
+    if(lane == 0) m_in = 0.0;
+    for(int j = 0; j < K; ++j) {
+      const double v = line[j * 32 + lane] + __ldg(&sa.fB[j * 32 + lane]) * m_in;
+      line[j * 32 + lane] = v;  // m_q
+    }
+    // back substitution, lane-local: x_{pK+j} = C_j + gD_j x_in
+    double cacc = 0.0;
+    for(int j = K - 1; j >= 0; --j) {
+      const double mq = line[j * 32 + lane];
+      cacc = j == K - 1 ? mq : mq - __ldg(&sa.cu[j * 32 + lane]) * cacc;
+      line[j * 32 + lane] = cacc;  // C_j
+    }
+    double bval = cacc;
+#pragma unroll
+    for(int s = 0; s < 5; ++s) {
+      const double dn = __shfl_down_sync(0xffffffffu, bval, 1 << s);
+      bval += __ldg(&sa.mb[s * 32 + lane]) * dn;
+    }
+    double x_in = __shfl_down_sync(0xffffffffu, bval, 1);
+    if(lane == 31) x_in = 0.0;
+    double x0 = 0.0, xl = 0.0;
+    for(int j = 0; j < K; ++j) {
+      const double x = line[j * 32 + lane] + __ldg(&sa.gD[j * 32 + lane]) * x_in;
+      line[j * 32 + lane] = x;
+      if(j == 0) x0 = x;
+      if(j == K - 1) xl = x;
+    }
+    if(a.periodic) {
+      const double first = __shfl_sync(0xffffffffu, x0, 0);
+      const double last = __shfl_sync(0xffffffffu, xl, 31);
+      const double factor = (first + a.uc_over_gamma * last) * a.inv_den;
+      for(int j = 0; j < K; ++j) line[j * 32 + lane] -= factor * __ldg(&sa.z[j * 32 + lane]);
+    }
+  }
+  __syncthreads();
+  if(XLINES) {
+    bool ok;
+    const int base = line_base(wl, ok);
+    if(ok) {
+      for(int q = lane; q < n; q += 32) out[base + q] = tile[slot(wl, q)];
+      if(a.copy_duplicate && lane == 0) out[base - a.begin * st + a.dup_index * st] = tile[slot(wl, 0)];
+    }
+  } else {
+    const int l = tid % LB;
+    bool ok;
+    const int base = line_base(l, ok);
+    if(ok) {
+      for(int q = tid / LB; q < n; q += 512 / LB) out[base + q * st] = tile[slot(l, q)];
+      if(a.copy_duplicate && tid < LB) out[base - a.begin * st + a.dup_index * st] = tile[slot(l, 0)];
+    }
+  }
+}
+
 }  // namespace
 
 void launch_adi_sweep(const AdiPlan* p, int comp, int axis, const double* in, double* out,
@@ -273,11 +594,53 @@ void launch_adi_sweep(const AdiPlan* p, int comp, int axis, const double* in, do
   a.z = p->coef + A.off + 2 * A.n;
   const int a1 = axis == 0 ? 1 : 0;
   const int a2 = axis == 2 ? 1 : 2;
-  dim3 block(128, 1, 1);
-  dim3 grid((a.L.n(a1) + 127) / 128, a.L.n(a2), 1);
   ProfScope ps(kKAdi, s);
-  k_adi_sweep<<<grid, block, 0, s>>>(a, in, out);
-  OFB_LAUNCH_CHECK("k_adi_sweep");
+  if(A.partition) {
+    ScanArgs sa;
+    sa.K = A.seg;
+    const int KP = A.seg * 32;
+    const double* base = p->coef + A.poff;
+    sa.ip = base;
+    sa.fB = base + KP;
+    sa.cu = base + 2 * KP;
+    sa.gD = base + 3 * KP;
+    sa.z = base + 4 * KP;
+    sa.mf = base + 5 * KP;
+    sa.mb = base + 5 * KP + 5 * 32;
+    const size_t smem = static_cast<size_t>(16) * (a.n + 1) * sizeof(double);
+    dim3 block(32, 16, 1);
+    if(axis == 0) {
+      const long long nl = static_cast<long long>(a.L.n(a1)) * a.L.n(a2);
+      dim3 grid(static_cast<unsigned>((nl + 15) / 16), 1, 1);
+      OFB_CHECK(cudaFuncSetAttribute(k_adi_scan<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(smem)));
+      k_adi_scan<true><<<grid, block, smem, s>>>(a, sa, in, out);
+    } else {
+      dim3 grid((a.L.n(a1) + 15) / 16, a.L.n(a2), 1);
+      OFB_CHECK(cudaFuncSetAttribute(k_adi_scan<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(smem)));
+      k_adi_scan<false><<<grid, block, smem, s>>>(a, sa, in, out);
+    }
+    OFB_LAUNCH_CHECK("k_adi_scan");
+    return;
+  }
+  // lines per warp so that one tile fits kAdiTileBytes (32 when n <= 255)
+  int lines = 32;
+  while(lines > 1 && static_cast<size_t>(lines) * (a.n + 1) * sizeof(double) > kAdiTileBytes) lines /= 2;
+  const size_t smem = static_cast<size_t>(lines) * (a.n + 1) * sizeof(double);
+  if(axis == 0) {
+    const long long nl = static_cast<long long>(a.L.n(a1)) * a.L.n(a2);
+    dim3 grid(static_cast<unsigned>((nl + lines - 1) / lines), 1, 1);
+    OFB_CHECK(cudaFuncSetAttribute(k_adi_tile<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(smem)));
+    k_adi_tile<true><<<grid, 32, smem, s>>>(a, in, out, lines);
+  } else {
+    dim3 grid((a.L.n(a1) + lines - 1) / lines, a.L.n(a2), 1);
+    OFB_CHECK(cudaFuncSetAttribute(k_adi_tile<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(smem)));
+    k_adi_tile<false><<<grid, 32, smem, s>>>(a, in, out, lines);
+  }
+  OFB_LAUNCH_CHECK("k_adi_tile");
 }
 
 }  // namespace ofb

@@ -21,45 +21,50 @@ __device__ __forceinline__ double safe_ratio(double num, double den) {
   return fabs(den) < kSmallDenominator ? 0.0 : num / den;
 }
 
-// reconstruct_face_{x,y,z} (solver/momentum_terms.cpp:42-151) for the face
-// whose upper ("right") cell is q, along an axis with storage stride st;
-// `ri` is the right cell's storage index on that axis and `smax` the last
-// storage index.  Faces within two cells of the storage bounds fall back to
-// first-order upwind, as in the reference.
-__device__ __forceinline__ double reconstruct(const double* __restrict__ f, int q, int st, int ri,
-                                              int smax, double vel) {
-  const double left = f[q - st];
-  const double right = f[q];
-  if(fabs(vel) < kSmallDenominator) return vel >= 0.0 ? left : right;
-  if(vel >= 0.0) {
-    if(ri - 2 < 0) return left;
-    const double delta_down = right - left;
-    const double ratio = safe_ratio(left - f[q - 2 * st], delta_down);
-    return left + 0.5 * van_leer(ratio) * delta_down;
-  }
-  if(ri + 1 > smax) return right;
+// Branch-free form of one reconstruct_face call: every candidate value is
+// loaded before the velocity sign is known and the reference's three cases
+// (first-order upwind for |u_f| < 1e-14 or near the storage bounds, van Leer
+// MUSCL otherwise; solver/momentum_terms.cpp:42-151) are chosen by selects.
+__device__ __forceinline__ double tvd_face(double vel, double left, double right, double far_left,
+                                           bool far_left_ok, double far_right, bool far_right_ok) {
+  const bool up = vel >= 0.0;
   const double delta = right - left;
-  const double ratio = safe_ratio(f[q + st] - right, delta);
-  return right - 0.5 * van_leer(ratio) * delta;
+  const double num = up ? left - far_left : far_right - right;
+  const double ratio = fabs(delta) < kSmallDenominator ? 0.0 : num / delta;
+  const double a = fabs(ratio);
+  const double phi = (ratio + a) / (1.0 + a);
+  const double muscl = up ? left + 0.5 * phi * delta : right - 0.5 * phi * delta;
+  const bool first_order = fabs(vel) < kSmallDenominator || (up ? !far_left_ok : !far_right_ok);
+  return first_order ? (up ? left : right) : muscl;
 }
 
 // compute_{u,v,w}_advection (solver/momentum_terms.cpp:153-266) at storage
-// point (i, j, k) of component C.
+// point (i, j, k) of component C, branch-free.
 template <int C>
-__device__ __forceinline__ double advection_at(const Grid& g, const double* __restrict__ const* vel,
-                                               int i, int j, int k, const double (&inv_h)[3]) {
+__device__ __forceinline__ double advection_bf(const Grid& g, const double* __restrict__ u,
+                                               const double* __restrict__ v,
+                                               const double* __restrict__ w, int i, int j, int k,
+                                               const double (&inv_h)[3]) {
+  const double* __restrict__ vel[3] = {u, v, w};
   const Lay L = make_lay(g, kFaceX + C);
   const double* __restrict__ f = vel[C];
   const int q = L.idx(i, j, k);
   const int pos[3] = {i, j, k};
+  const double f0 = f[q];
   double flux_div = 0.0;
 #pragma unroll
   for(int d = 0; d < 3; ++d) {
+    const int st = L.stride(d);
+    const int smax = L.s(d) - 1;
+    const int pd = pos[d];
+    const double fm1 = f[q - st];
+    const double fp1 = f[q + st];
+    const double fm2 = f[pd - 2 >= 0 ? q - 2 * st : q - st];
+    const double fp2 = f[pd + 2 <= smax ? q + 2 * st : q + st];
     double lo_vel, hi_vel;
-    const int std_ = L.stride(d);
     if(d == C) {
-      lo_vel = 0.5 * (f[q - std_] + f[q]);
-      hi_vel = 0.5 * (f[q] + f[q + std_]);
+      lo_vel = 0.5 * (fm1 + f0);
+      hi_vel = 0.5 * (f0 + fp1);
     } else {
       const Lay D = make_lay(g, kFaceX + d);
       const double* __restrict__ fd = vel[d];
@@ -71,16 +76,36 @@ __device__ __forceinline__ double advection_at(const Grid& g, const double* __re
       lo_vel = 0.5 * (fd[qdm] + fd[qd]);
       hi_vel = 0.5 * (fd[qdm + sd] + fd[qd + sd]);
     }
-    const int smax = L.s(d) - 1;
-    const double lo_flux = lo_vel * reconstruct(f, q, std_, pos[d], smax, lo_vel);
-    const double hi_flux = hi_vel * reconstruct(f, q + std_, std_, pos[d] + 1, smax, hi_vel);
-    flux_div += (hi_flux - lo_flux) * inv_h[d];
+    const double lo_face = tvd_face(lo_vel, fm1, f0, fm2, pd - 2 >= 0, fp1, pd + 1 <= smax);
+    const double hi_face = tvd_face(hi_vel, f0, fp1, fm1, pd - 1 >= 0, fp2, pd + 2 <= smax);
+    flux_div += (hi_vel * hi_face - lo_vel * lo_face) * inv_h[d];
   }
   return flux_div;
 }
 
+// Advection term of component C at every active point, written to adv[C]
+// (the first half of assemble_predictor_rhs, solver/taylor_green.cpp:238).
 template <int C>
-__global__ void __launch_bounds__(kTX* kTY) k_predictor_rhs(PredictorArgs a, int kchunk) {
+__global__ void __launch_bounds__(kTX* kTY)
+    k_advect_bf(Grid g, const double* __restrict__ u, const double* __restrict__ v,
+                const double* __restrict__ w, double* __restrict__ out, int kchunk) {
+  const Lay L = make_lay(g, kFaceX + C);
+  const int i = blockIdx.x * kTX + threadIdx.x + 1;
+  const int j = blockIdx.y * kTY + threadIdx.y + 1;
+  if(i > L.nx || j > L.ny) return;
+  const int k0 = blockIdx.z * kchunk + 1;
+  const int k1 = min(k0 + kchunk, L.nz + 1);
+  const double inv_h[3] = {1.0 / g.dx, 1.0 / g.dy, 1.0 / g.dz};
+  for(int k = k0; k < k1; ++k) out[L.idx(i, j, k)] = advection_bf<C>(g, u, v, w, i, j, k, inv_h);
+}
+
+// The rest of assemble_predictor_rhs (solver/taylor_green.cpp:239-255):
+// diffusion, total-pressure gradient, factorisation correction and the AB2
+// combination with the advection term computed by k_advect_bf.  The 27-point
+// correction is evaluated column by column (second z-differences first), so
+// only 18 neighbourhood values are live at once.
+template <int C>
+__global__ void __launch_bounds__(kTX* kTY) k_predictor_rest(PredictorArgs a, int kchunk) {
   const Grid& g = a.g;
   const Lay L = make_lay(g, kFaceX + C);
   const Lay P = make_lay(g, kCell);
@@ -89,7 +114,7 @@ __global__ void __launch_bounds__(kTX* kTY) k_predictor_rhs(PredictorArgs a, int
   if(i > L.nx || j > L.ny) return;
   const int k0 = blockIdx.z * kchunk + 1;
   const int k1 = min(k0 + kchunk, L.nz + 1);
-  const double inv_h[3] = {1.0 / g.dx, 1.0 / g.dy, 1.0 / g.dz};
+  const double ih = 1.0 / g.h(C);
   const double ix = 1.0 / (g.dx * g.dx), iy = 1.0 / (g.dy * g.dy), iz = 1.0 / (g.dz * g.dz);
   const double dy2 = g.dy * g.dy;
   const bool three_d = g.nz != 1;
@@ -99,83 +124,61 @@ __global__ void __launch_bounds__(kTX* kTY) k_predictor_rhs(PredictorArgs a, int
   const double s_prev = 0.5 * a.dt;
   const double s_corr = a.alpha * a.alpha;
   const double* __restrict__ f = a.cur[C];
-  const int stC = L.stride(C);
   const int pstC = P.stride(C);
   for(int k = k0; k < k1; ++k) {
     const int q = L.idx(i, j, k);
-    // 27-point neighbourhood v[dz][dy][dx]
-    double v[3][3][3];
+    // in-plane values m[dy][dx] and second z-differences z2[dy][dx]
+    double m[3][3], z2[3][3];
+    double fzm = 0.0, fzp = 0.0;
 #pragma unroll
-    for(int c = 0; c < 3; ++c)
+    for(int b = 0; b < 3; ++b)
 #pragma unroll
-      for(int b = 0; b < 3; ++b)
-#pragma unroll
-        for(int e = 0; e < 3; ++e) v[c][b][e] = f[q + (e - 1) + (b - 1) * L.sx + (c - 1) * L.sxy];
-
-    const double adv = advection_at<C>(g, a.cur, i, j, k, inv_h);
-    // compute_diffusion_term: (d2x + d2y + d2z) * nu
-    const double c2 = 2.0 * v[1][1][1];
-    const double lap = (v[1][1][2] - c2 + v[1][1][0]) * ix + (v[1][2][1] - c2 + v[1][0][1]) * iy +
-                       (v[2][1][1] - c2 + v[0][1][1]) * iz;
+      for(int e = 0; e < 3; ++e) {
+        const int qq = q + (e - 1) + (b - 1) * L.sx;
+        const double lo = f[qq - L.sxy], mid = f[qq], hi = f[qq + L.sxy];
+        m[b][e] = mid;
+        z2[b][e] = (hi - 2.0 * mid + lo) * iz;
+        if(b == 1 && e == 1) {
+          fzm = lo;
+          fzp = hi;
+        }
+      }
+    const double c2 = 2.0 * m[1][1];
+    const double lap = (m[1][2] - c2 + m[1][0]) * ix + (m[2][1] - c2 + m[0][1]) * iy +
+                       (fzp - c2 + fzm) * iz;
     const double dif = lap * a.nu;
-    // compute_gradient of the total pressure onto this face
-    int pc[3] = {i, j, k};
-    const int pq = P.idx(pc[0], pc[1], pc[2]);
-    const double gp = (a.p[pq] - a.p[pq - pstC]) * inv_h[C];
-    // factorisation correction (solver/taylor_green.cpp:196-225,
-    // solver/lid_driven_cavity.cpp:219-252)
+    const int pq = P.idx(i, j, k);
+    const double gp = (a.p[pq] - a.p[pq - pstC]) * ih;
     double corr;
     if(a.variant == 1) {
       double dyy[3];
 #pragma unroll
-      for(int e = 0; e < 3; ++e) dyy[e] = (v[1][2][e] - 2.0 * v[1][1][e] + v[1][0][e]) / dy2;
+      for(int e = 0; e < 3; ++e) dyy[e] = (m[2][e] - 2.0 * m[1][e] + m[0][e]) / dy2;
       corr = (dyy[2] - 2.0 * dyy[1] + dyy[0]) * ix;
     } else {
       double d2y[3];
 #pragma unroll
-      for(int e = 0; e < 3; ++e) d2y[e] = (v[1][2][e] - 2.0 * v[1][1][e] + v[1][0][e]) * iy;
+      for(int e = 0; e < 3; ++e) d2y[e] = (m[2][e] - 2.0 * m[1][e] + m[0][e]) * iy;
       corr = (d2y[2] - 2.0 * d2y[1] + d2y[0]) * ix;
       if(three_d) {
-        double d2z[3][3];  // [dy][dx]
-#pragma unroll
-        for(int b = 0; b < 3; ++b)
-#pragma unroll
-          for(int e = 0; e < 3; ++e) d2z[b][e] = (v[2][b][e] - 2.0 * v[1][b][e] + v[0][b][e]) * iz;
-        const double mxz = (d2z[1][2] - 2.0 * d2z[1][1] + d2z[1][0]) * ix;
+        const double mxz = (z2[1][2] - 2.0 * z2[1][1] + z2[1][0]) * ix;
         double myz[3];
 #pragma unroll
-        for(int e = 0; e < 3; ++e) myz[e] = (d2z[2][e] - 2.0 * d2z[1][e] + d2z[0][e]) * iy;
+        for(int e = 0; e < 3; ++e) myz[e] = (z2[2][e] - 2.0 * z2[1][e] + z2[0][e]) * iy;
         const double triple = (myz[2] - 2.0 * myz[1] + myz[0]) * ix;
         corr += mxz;
         corr += myz[1];
         corr -= a.alpha * triple;
       }
     }
-    // assemble_predictor_rhs (solver/taylor_green.cpp:244-255)
-    double r = v[1][1][1];
+    double r = m[1][1];
     r += s_gp * gp;
     r += s_dif * dif;
-    r += s_adv * adv;
+    r += s_adv * a.adv[C][q];
     if(a.has_prev) r += s_prev * a.prev[C][q];
     r += s_corr * corr;
-    a.adv[C][q] = adv;
     a.rhs[C][q] = r;
-    (void)stC;
   }
-}
-
-template <int C>
-__global__ void __launch_bounds__(kTX* kTY) k_advection(Grid g, const double* u, const double* v,
-                                                        const double* w, double* out, int kchunk) {
-  const Lay L = make_lay(g, kFaceX + C);
-  const int i = blockIdx.x * kTX + threadIdx.x + 1;
-  const int j = blockIdx.y * kTY + threadIdx.y + 1;
-  if(i > L.nx || j > L.ny) return;
-  const int k0 = blockIdx.z * kchunk + 1;
-  const int k1 = min(k0 + kchunk, L.nz + 1);
-  const double inv_h[3] = {1.0 / g.dx, 1.0 / g.dy, 1.0 / g.dz};
-  const double* vel[3] = {u, v, w};
-  for(int k = k0; k < k1; ++k) out[L.idx(i, j, k)] = advection_at<C>(g, vel, i, j, k, inv_h);
 }
 
 // initialize_exact_state (solver/taylor_green.cpp:335-395), active entries.
@@ -209,16 +212,23 @@ __global__ void k_tg_init(Grid g, int mode, int loc, double* f) {
 
 void launch_predictor_rhs(const PredictorArgs& a, cudaStream_t s) {
   const Lay Lu = make_lay(a.g, kFaceX), Lv = make_lay(a.g, kFaceY), Lw = make_lay(a.g, kFaceZ);
-  ProfScope ps(kKPredictor, s, 3);
-  Launch3 l0 = launch3(Lu.nx, Lu.ny, Lu.nz);
-  k_predictor_rhs<0><<<l0.grid, l0.block, 0, s>>>(a, l0.kchunk);
-  OFB_LAUNCH_CHECK("k_predictor_rhs<0>");
-  Launch3 l1 = launch3(Lv.nx, Lv.ny, Lv.nz);
-  k_predictor_rhs<1><<<l1.grid, l1.block, 0, s>>>(a, l1.kchunk);
-  OFB_LAUNCH_CHECK("k_predictor_rhs<1>");
-  Launch3 l2 = launch3(Lw.nx, Lw.ny, Lw.nz);
-  k_predictor_rhs<2><<<l2.grid, l2.block, 0, s>>>(a, l2.kchunk);
-  OFB_LAUNCH_CHECK("k_predictor_rhs<2>");
+  const Launch3 l0 = launch3(Lu.nx, Lu.ny, Lu.nz);
+  const Launch3 l1 = launch3(Lv.nx, Lv.ny, Lv.nz);
+  const Launch3 l2 = launch3(Lw.nx, Lw.ny, Lw.nz);
+  {
+    ProfScope ps(kKAdvection, s, 3);
+    k_advect_bf<0><<<l0.grid, l0.block, 0, s>>>(a.g, a.cur[0], a.cur[1], a.cur[2], a.adv[0], l0.kchunk);
+    k_advect_bf<1><<<l1.grid, l1.block, 0, s>>>(a.g, a.cur[0], a.cur[1], a.cur[2], a.adv[1], l1.kchunk);
+    k_advect_bf<2><<<l2.grid, l2.block, 0, s>>>(a.g, a.cur[0], a.cur[1], a.cur[2], a.adv[2], l2.kchunk);
+    OFB_LAUNCH_CHECK("k_advect_bf");
+  }
+  {
+    ProfScope ps(kKPredictor, s, 3);
+    k_predictor_rest<0><<<l0.grid, l0.block, 0, s>>>(a, l0.kchunk);
+    k_predictor_rest<1><<<l1.grid, l1.block, 0, s>>>(a, l1.kchunk);
+    k_predictor_rest<2><<<l2.grid, l2.block, 0, s>>>(a, l2.kchunk);
+    OFB_LAUNCH_CHECK("k_predictor_rest");
+  }
 }
 
 void launch_advection(const Grid& g, const double* u, const double* v, const double* w,
@@ -226,11 +236,11 @@ void launch_advection(const Grid& g, const double* u, const double* v, const dou
   const Lay Lu = make_lay(g, kFaceX), Lv = make_lay(g, kFaceY), Lw = make_lay(g, kFaceZ);
   ProfScope ps(kKOther, s, 3);
   Launch3 l0 = launch3(Lu.nx, Lu.ny, Lu.nz);
-  k_advection<0><<<l0.grid, l0.block, 0, s>>>(g, u, v, w, au, l0.kchunk);
+  k_advect_bf<0><<<l0.grid, l0.block, 0, s>>>(g, u, v, w, au, l0.kchunk);
   Launch3 l1 = launch3(Lv.nx, Lv.ny, Lv.nz);
-  k_advection<1><<<l1.grid, l1.block, 0, s>>>(g, u, v, w, av, l1.kchunk);
+  k_advect_bf<1><<<l1.grid, l1.block, 0, s>>>(g, u, v, w, av, l1.kchunk);
   Launch3 l2 = launch3(Lw.nx, Lw.ny, Lw.nz);
-  k_advection<2><<<l2.grid, l2.block, 0, s>>>(g, u, v, w, aw, l2.kchunk);
+  k_advect_bf<2><<<l2.grid, l2.block, 0, s>>>(g, u, v, w, aw, l2.kchunk);
   OFB_LAUNCH_CHECK("k_advection");
 }
 

@@ -48,7 +48,7 @@ cudaEvent_t take_event(Profiler& p) {
 }
 
 const char* kNames[kKernelCount] = {
-    "predictor_rhs", "adi_sweep", "velocity_bc", "divergence_rhs", "pcg_initial_residual",
+    "predictor_rhs", "advection", "adi_sweep", "velocity_bc", "divergence_rhs", "pcg_initial_residual",
     "pcg_apply_ap", "pcg_update_xr", "pcg_update_p", "vcycle_smooth_first_fine",
     "vcycle_smooth_fine", "vcycle_restrict_fine", "vcycle_prolong_smooth_fine",
     "vcycle_coarse_levels", "vcycle_coarse_solve", "correct_velocity", "cell_pass",

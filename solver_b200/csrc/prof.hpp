@@ -7,6 +7,7 @@ namespace ofb {
 
 enum KernelClass : int {
   kKPredictor = 0,
+  kKAdvection,
   kKAdi,
   kKVelocityBc,
   kKDivergence,

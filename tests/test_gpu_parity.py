@@ -110,6 +110,28 @@ def test_predictor_adi_matches_oracle(sb, oracle, types):
         assert rel_maxdiff(a, b) <= OP_TOL
 
 
+@pytest.mark.parametrize("types", [
+    [po.PERIODIC] * 6,
+    [po.NO_SLIP_WALL, po.NO_SLIP_WALL, po.NO_SLIP_WALL, po.PRESCRIBED_VELOCITY, po.SYMMETRY,
+     po.SYMMETRY],
+    [po.PERIODIC, po.PERIODIC, po.NO_SLIP_WALL, po.PRESCRIBED_VELOCITY, po.PERIODIC, po.PERIODIC],
+])
+def test_predictor_adi_partition_solver_matches_oracle(sb, oracle, types):
+    """Lines of 64 and 96 unknowns take the warp-per-line partition solver."""
+    rng = np.random.default_rng(5)
+    g = po.Grid(64, 96, 64, 0.02, 0.03, 0.025)
+    vel = [None] * 6
+    vel[3] = (0.7, 0.0, 0.1)
+    bc = po.bc_from(types, vel)
+    rhs = _random_velocity(g, rng)
+    ctx = sb.Context(to_gpu_grid(g), to_gpu_bc(bc))
+    got, lines = ctx.solve_predictor_adi(rhs, 0.3)
+    exp, lines_ref = oracle.predictor_adi(g, bc, 0.3, *rhs)
+    assert lines == lines_ref
+    for a, b in zip(got, exp):
+        assert rel_maxdiff(a, b) <= OP_TOL
+
+
 @pytest.mark.parametrize("case", ["dirichlet2d", "neumann2d", "periodic3d", "mixed3d",
                                   "mixed3d_tiled"])
 def test_poisson_matches_oracle(sb, oracle, case):
