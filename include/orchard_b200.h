@@ -218,6 +218,39 @@ of_status of_tg_init(of_ctx* ctx, double viscosity, double dt, int mode);
 of_status of_run_steps(of_ctx* ctx, const of_step_params* params, int steps,
                        of_step_metrics* metrics);
 
+/* ---- allocation-free entry point ---------------------------------------- */
+
+/* No counterpart in the reference (it has no device path).  The pressure
+ * right-hand side pass of project_velocity on DEVICE buffers, without a
+ * context: pressure_rhs = (density/dt) div(u) on the active cells
+ * (build_pressure_rhs, solver/projection.cpp:1049-1064) and, when norms is
+ * not NULL, norms[0] = divergence_l2_before and norms[1] = rhs_l2 (host
+ * doubles; solver/projection.cpp:1110-1116).
+ *
+ * For callers that cannot allocate device memory: a framework that owns all
+ * device memory through its own pool and calls this inside its step loop,
+ * where a context's allocations and the device-wide synchronisation of
+ * cudaMalloc/cudaFree are not acceptable.  The call allocates nothing: its
+ * scratch (reduction partials, ticket, norms; 131,104 bytes) is a static
+ * device array of the library, found by cudaGetSymbolAddress on the first
+ * call on each device (setup; make that first call before any stream capture).
+ *
+ *  - u, v, w: device face fields in padded storage whose boundary conditions
+ *    are already applied (project_velocity's `working` after
+ *    apply_velocity_boundary_conditions); only active faces are read.
+ *  - pressure_rhs: device cell field; active entries written, ghosts untouched.
+ *  - Runs on the current CUDA device and on `stream` (a cudaStream_t; NULL is
+ *    the default stream).  With norms == NULL the call only enqueues work;
+ *    otherwise it returns after the norms are on the host.
+ *  - Limits: at most 8192 blocks of 32 x 8 cells per k plane
+ *    (ceil(nx/32) * ceil(ny/8) <= 8192, i.e. 2,097,152 cells per plane) and
+ *    (nx+3)(ny+3)(nz+3) < 2^31; larger grids fail with OF_INVALID_ARGUMENT.
+ *  - Calls on one device share the scratch: calls that overlap in time (two
+ *    streams, two host threads) race and give wrong norms.  Serialise them. */
+of_status of_pressure_rhs_noalloc(const of_grid* grid, double dt, double density,
+                                  const double* u, const double* v, const double* w,
+                                  double* pressure_rhs, double* norms, void* stream);
+
 /* ---- instrumentation ---------------------------------------------------- */
 
 /* The context's CUDA stream (cudaStream_t) for callers that time on it. */

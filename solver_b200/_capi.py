@@ -109,6 +109,9 @@ def load():
         lib.of_run_steps.argtypes = [C.c_void_p, C.POINTER(OfStepParams), C.c_int,
                                      C.POINTER(OfStepMetrics)]
         lib.of_stream.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
+        # device pointers (u, v, w, pressure_rhs, stream) as c_void_p
+        lib.of_pressure_rhs_noalloc.argtypes = [C.POINTER(OfGrid), C.c_double, C.c_double] + \
+            [C.c_void_p] * 4 + [DP, C.c_void_p]
         lib.of_kernel_class_name.restype = C.c_char_p
         lib.of_profile_enable.argtypes = [C.c_int]
         lib.of_profile_read.argtypes = [C.c_int, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),

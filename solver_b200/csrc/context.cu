@@ -682,4 +682,42 @@ of_status of_run_steps(of_ctx* ctx, const of_step_params* prm, int steps, of_ste
   });
 }
 
+// Allocation-free pressure rhs for callers whose device memory is owned by
+// their own allocator and who cannot let a call allocate or synchronise the
+// device inside their step loop (ofb::launch_pressure_rhs_noalloc, noalloc.cu).
+of_status of_pressure_rhs_noalloc(const of_grid* grid, double dt, double density,
+                                  const double* u, const double* v, const double* w,
+                                  double* pressure_rhs, double* norms, void* stream) {
+  return guarded([&] {
+    require_ptr(grid, "grid");
+    require_ptr(u, "velocity u");
+    require_ptr(v, "velocity v");
+    require_ptr(w, "velocity w");
+    require_ptr(pressure_rhs, "pressure rhs");
+    if(grid->nx <= 0 || grid->ny <= 0 || grid->nz <= 0)
+      fail(OF_INVALID_ARGUMENT, "grid dimensions must be positive");
+    if(grid->dx <= 0.0 || grid->dy <= 0.0 || grid->dz <= 0.0)
+      fail(OF_INVALID_ARGUMENT, "grid spacing must be positive");
+    const long long cells = static_cast<long long>(grid->nx + 3) * (grid->ny + 3) * (grid->nz + 3);
+    if(cells >= (1LL << 31)) fail(OF_INVALID_ARGUMENT, "grid too large for 32-bit indexing");
+    // the scratch holds the block partials of one launch; a launch has
+    // ceil(nx/32) * ceil(ny/8) blocks per k plane at least
+    const long long plane_blocks = static_cast<long long>((grid->nx + ofb::kTX - 1) / ofb::kTX) *
+                                   ((grid->ny + ofb::kTY - 1) / ofb::kTY);
+    if(plane_blocks > ofb::noalloc_max_plane_blocks()) {
+      std::ostringstream m;
+      m << "of_pressure_rhs_noalloc: a " << grid->nx << " x " << grid->ny
+        << " k plane needs " << plane_blocks << " reduction blocks of 32 x 8 cells; the static "
+        << "scratch holds " << ofb::noalloc_max_plane_blocks() << " (at most "
+        << ofb::noalloc_max_plane_blocks() * ofb::kTX * ofb::kTY << " cells per k plane)";
+      fail(OF_INVALID_ARGUMENT, m.str());
+    }
+    if(dt <= 0.0) fail(OF_INVALID_ARGUMENT, "build_pressure_rhs expects dt > 0");
+    if(density <= 0.0) fail(OF_INVALID_ARGUMENT, "build_pressure_rhs expects density > 0");
+    const Grid g{grid->nx, grid->ny, grid->nz, grid->dx, grid->dy, grid->dz};
+    ofb::launch_pressure_rhs_noalloc(g, u, v, w, density / dt, pressure_rhs, ofb::noalloc_scratch(),
+                                     norms, static_cast<cudaStream_t>(stream));
+  });
+}
+
 }  // extern "C"

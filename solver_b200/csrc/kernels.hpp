@@ -142,4 +142,17 @@ void poisson_solve(PoissonPlan* p, int max_iterations, double tolerance, SolveSc
 void launch_compact_to_pressure(const Grid& g, const double* x, const SolveScalars* sc,
                                 double* p_padded, cudaStream_t s);
 
+// ---- allocation-free pressure rhs (noalloc.cu) ----
+// Device address of the file-scope scratch on the current device (looked up
+// once per device with cudaGetSymbolAddress, then cached).
+double* noalloc_scratch();
+// Most reduction blocks the scratch holds for one k plane (32 x 8 cells each).
+long long noalloc_max_plane_blocks();
+// rhs = scale div(u) on the active cells of a padded cell field, plus
+// norms_host[0] = divergence L2, norms_host[1] = rhs L2 (active means) when
+// norms_host != nullptr, in which case the stream is synchronised.
+void launch_pressure_rhs_noalloc(const Grid& g, const double* u, const double* v, const double* w,
+                                 double scale, double* rhs, double* scratch, double* norms_host,
+                                 cudaStream_t s);
+
 }  // namespace ofb
