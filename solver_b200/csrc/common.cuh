@@ -113,6 +113,7 @@ __host__ __device__ __forceinline__ bool is_dirichlet_velocity(int type) {
 constexpr int kTX = 32;
 constexpr int kTY = 8;
 constexpr int kMaxBlocks = 8192;
+constexpr int kTargetBlocks = 8 * 148;  // eight blocks per SM of a B200
 constexpr int kRedThreads = 256;
 
 struct Launch3 {

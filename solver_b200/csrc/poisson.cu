@@ -332,7 +332,7 @@ __host__ __device__ __forceinline__ bool vfits(const CLay& L) {
 }
 
 // Vector kernels can be switched off for comparisons: ORCHARD_B200_NO_VEC=1
-// (all) or a comma list of smooth, prolong, restrict, ap.  Read at each use so
+// (all) or a comma list of smooth, pre, prolong, restrict, ap.  Read at each use so
 // that a process can compare both forms.
 bool vec_enabled(const char* which = "") {
   const char* e = std::getenv("ORCHARD_B200_NO_VEC");
@@ -404,6 +404,57 @@ __global__ void __launch_bounds__(256)
         sc->rz = rz_new;
       }
     }
+  });
+}
+
+// Both pre-smoothing sweeps from a zero correction in one pass over b: the
+// first sweep is pointwise, a = omega (b - sb) / D, so the second one,
+// out = a + omega (b - sb - A a) / D, reads b alone (a is formed on load for
+// every neighbour).  The reference removes mean(a) between the sweeps; A
+// annihilates constants on the problems where it does that (periodic /
+// all-Neumann), so the shift only moves out by a constant, which the mean
+// recorded here (ls->sx) removes as before.
+template <typename T, typename B>
+__global__ void __launch_bounds__(256)
+    k_vsmooth_pre(OpInfo o, const B* __restrict__ b, const double* sb_ptr, T* __restrict__ out,
+                  LevelScalars* ls, int zm, int kchunk, RedBuf rb) {
+  using A = T;
+  ROW_PROLOGUE(T)
+  using R = vst::Row<A, W>;
+  using RB = vst::Row<double, W>;
+  const double sb = *sb_ptr;
+  const A om = A(kOmega);
+  auto a_at = [&](int ii, int jj, int kk, double bv) {
+    return om * A(bv - sb) * A(inv_diag(o, ii, jj, kk));
+  };
+  double acc[1] = {0.0};
+  vst::march<A, W, RB>(
+      o, g, k0, k1,
+      [&](int i0, int jj, int kk) {
+        const RB bb = vst::ld<double, W>(b + o.L.idx(i0, jj, kk));
+        R r;
+#pragma unroll
+        for(int t = 0; t < W; ++t) r.v[t] = a_at(i0 + t, jj, kk, bb.v[t]);
+        return r;
+      },
+      [&](int ii, int jj, int kk) { return a_at(ii, jj, kk, double(b[o.L.idx(ii, jj, kk)])); },
+      [&](int i0, int jj, int kk) { return vst::ld<double, W>(b + o.L.idx(i0, jj, kk)); },
+      [&](int k, const R& c, const R& ax, const RB& bb) {
+        R v;
+#pragma unroll
+        for(int t = 0; t < W; ++t)
+          v.v[t] = c.v[t] + om * (A(bb.v[t] - sb) - ax.v[t]) * A(inv_diag(o, g.i0 + t, g.j, k));
+        if(g.act) {
+          vst::st<T, W>(out + o.L.idx(g.i0, g.j, k), v);
+#pragma unroll
+          for(int t = 0; t < W; ++t) acc[0] += double(v.v[t]);
+        }
+      });
+  const bool mx[1] = {false};
+  const int n = o.L.count();
+  reduce_finish<1>(acc, mx, rb, [=](const Sums<1>& s) {
+    ls->sx = zm ? s.v[0] / n : 0.0;
+    ls->sum_x = s.v[0];
   });
 }
 
@@ -678,6 +729,212 @@ __global__ void k_coarse_solve(int n, const int* __restrict__ swaps, const doubl
 }
 
 // ---------------------------------------------------------------------------
+// The small end of the hierarchy in one block.  From the first level of at
+// most kTailMaxCells cells down to the coarsest, v_cycle (:597-633) runs in
+// one 1024-thread block with every level's rhs, correction and scratch in
+// shared memory, and each mean removal of the reference (after every sweep,
+// on the residual, on the coarse rhs, after the prolongation) done exactly,
+// by a block reduction.  One launch replaces five launches per level, each of
+// which was mostly launch latency and a dependent-load chain.
+// ---------------------------------------------------------------------------
+constexpr int kTailMaxCells = 4096;
+constexpr int kTailMaxLevels = 12;
+constexpr int kTailThreads = 1024;
+
+struct TailLevel {
+  OpInfo op;
+  int sx, sy, sz;  // log2 of the refinement ratio to the next coarser level
+  int off;         // offset of the level's b, x, s arrays in shared memory (elements)
+};
+
+struct TailArgs {
+  int count;  // levels in the tail; the last one is the coarsest
+  TailLevel lv[kTailMaxLevels];
+  int coarse_n;
+  int coarse_off;  // offset (elements, 8-byte aligned) of the FP64 solve vector
+  const int* swaps;
+  const double* factors;
+  int zm;
+};
+
+// Block-wide sum; every thread gets the same total (fixed order).
+__device__ __forceinline__ double tail_sum(double v, double* red) {
+  v = warp_sum(v);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if(lane == 0) red[warp] = v;
+  __syncthreads();
+  double s = 0.0;
+  const int nw = (blockDim.x + 31) >> 5;
+  for(int w = 0; w < nw; ++w) s += red[w];
+  __syncthreads();
+  return s;
+}
+
+__device__ __forceinline__ void tail_coords(const CLay& L, int q, int& i, int& j, int& k) {
+  k = q / L.nxy;
+  const int r = q - k * L.nxy;
+  j = r / L.nx;
+  i = r - j * L.nx;
+}
+
+// smooth_jacobi, one sweep: x <- x + omega (b - A x) / D, then x - mean(x).
+template <typename A>
+__device__ void tail_sweep(const OpInfo& o, const A* b, A* x, A* s, int zm, double* red) {
+  const int n = o.L.count();
+  double part = 0.0;
+  for(int q = threadIdx.x; q < n; q += blockDim.x) {
+    int i, j, k;
+    tail_coords(o.L, q, i, j, k);
+    const ColNb nb = col_nb(o, i, j);
+    A c;
+    const A ax = apply_op<A>(o, nb, i, j, k, [&](int ii, int jj, int kk) { return x[o.L.idx(ii, jj, kk)]; }, c);
+    const A v = c + A(kOmega) * (b[q] - ax) * A(inv_diag(o, i, j, k));
+    s[q] = v;
+    part += double(v);
+  }
+  const double sum = tail_sum(part, red);
+  const A mean = zm ? A(sum / n) : A(0);
+  for(int q = threadIdx.x; q < n; q += blockDim.x) x[q] = s[q] - mean;
+  __syncthreads();
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kTailThreads)
+    k_vcycle_tail(TailArgs a, const T* __restrict__ b_in, const double* sb_ptr, T* __restrict__ x_out,
+                  LevelScalars* ls_out) {
+  using A = T;
+  extern __shared__ __align__(16) unsigned char tail_smem[];
+  A* sm = reinterpret_cast<A*>(tail_smem);
+  __shared__ double red[32];
+  const int tid = threadIdx.x, bd = blockDim.x;
+  const int zm = a.zm;
+  auto B = [&](int l) { return sm + a.lv[l].off; };
+  auto X = [&](int l) { return sm + a.lv[l].off + a.lv[l].op.L.count(); };
+  auto S = [&](int l) { return sm + a.lv[l].off + 2 * a.lv[l].op.L.count(); };
+  {
+    const double sb = *sb_ptr;
+    const int n0 = a.lv[0].op.L.count();
+    for(int q = tid; q < n0; q += bd) B(0)[q] = A(double(b_in[q]) - sb);
+  }
+  __syncthreads();
+  const int last = a.count - 1;
+  // descent: pre-smoothing from zero, residual, restriction
+  for(int l = 0; l < last; ++l) {
+    const OpInfo& o = a.lv[l].op;
+    const int n = o.L.count();
+    A* b = B(l);
+    A* x = X(l);
+    A* s = S(l);
+    for(int q = tid; q < n; q += bd) x[q] = A(0);
+    __syncthreads();
+    tail_sweep<A>(o, b, x, s, zm, red);
+    tail_sweep<A>(o, b, x, s, zm, red);
+    double part = 0.0;
+    for(int q = tid; q < n; q += bd) {
+      int i, j, k;
+      tail_coords(o.L, q, i, j, k);
+      const ColNb nb = col_nb(o, i, j);
+      A c;
+      const A ax = apply_op<A>(o, nb, i, j, k, [&](int ii, int jj, int kk) { return x[o.L.idx(ii, jj, kk)]; }, c);
+      const A r = b[q] - ax;
+      s[q] = r;
+      part += double(r);
+    }
+    const double rsum = tail_sum(part, red);
+    const A mr = zm ? A(rsum / n) : A(0);
+    // restrict_full_weighting (:397-424), children in dz, dy, dx order
+    const CLay& Lc = a.lv[l + 1].op.L;
+    const int nc = Lc.count();
+    const int RX = 1 << a.lv[l].sx, RY = 1 << a.lv[l].sy, RZ = 1 << a.lv[l].sz;
+    const A inv_children = A(1.0 / double(RX * RY * RZ));
+    A* bc = B(l + 1);
+    double pc = 0.0;
+    for(int Q = tid; Q < nc; Q += bd) {
+      int I, J, K;
+      tail_coords(Lc, Q, I, J, K);
+      A sum = A(0);
+      for(int dz = 0; dz < RZ; ++dz)
+        for(int dy = 0; dy < RY; ++dy)
+          for(int dx = 0; dx < RX; ++dx)
+            sum += s[o.L.idx(I * RX + dx, J * RY + dy, K * RZ + dz)] - mr;
+      const A v = inv_children * sum;
+      bc[Q] = v;
+      pc += double(v);
+    }
+    const double csum = tail_sum(pc, red);
+    const A mc = zm ? A(csum / nc) : A(0);
+    for(int Q = tid; Q < nc; Q += bd) bc[Q] -= mc;
+    __syncthreads();
+  }
+  // direct_coarse_solve (:530-567): the host elimination replayed on the rhs
+  {
+    const int n = a.coarse_n;
+    A* y = B(last);
+    A* xc = X(last);
+    double* yd = reinterpret_cast<double*>(sm + a.coarse_off);  // solve in FP64
+    for(int q = tid; q < n; q += bd) yd[q] = double(y[q]);
+    __syncthreads();
+    if(zm && tid == 0) yd[n - 1] = 0.0;
+    __syncthreads();
+    for(int p = 0; p < n; ++p) {
+      if(tid == 0 && a.swaps[p] != p) {
+        const double tmp = yd[p];
+        yd[p] = yd[a.swaps[p]];
+        yd[a.swaps[p]] = tmp;
+      }
+      __syncthreads();
+      const double yp = yd[p];
+      for(int r = p + 1 + tid; r < n; r += bd) {
+        const double factor = a.factors[static_cast<size_t>(r) * n + p];
+        if(factor != 0.0) yd[r] -= factor * yp;
+      }
+      __syncthreads();
+    }
+    for(int row = n - 1; row >= 0; --row) {
+      if(tid == 0) yd[row] = yd[row] / a.factors[static_cast<size_t>(row) * n + row];
+      __syncthreads();
+      const double yr = yd[row];
+      for(int r = tid; r < row; r += bd) yd[r] -= a.factors[static_cast<size_t>(r) * n + row] * yr;
+      __syncthreads();
+    }
+    double part = 0.0;
+    for(int q = tid; q < n; q += bd) part += yd[q];
+    const double sum = tail_sum(part, red);
+    const double mean = zm ? sum / n : 0.0;
+    for(int q = tid; q < n; q += bd) xc[q] = A(yd[q] - mean);
+    __syncthreads();
+  }
+  // ascent: prolongate_and_add (:426-451), mean removal, post-smoothing
+  for(int l = last - 1; l >= 0; --l) {
+    const OpInfo& o = a.lv[l].op;
+    const int n = o.L.count();
+    A* x = X(l);
+    const A* xc = X(l + 1);
+    const CLay& Lc = a.lv[l + 1].op.L;
+    double part = 0.0;
+    for(int q = tid; q < n; q += bd) {
+      int i, j, k;
+      tail_coords(o.L, q, i, j, k);
+      const A v = x[q] + xc[Lc.idx(i >> a.lv[l].sx, j >> a.lv[l].sy, k >> a.lv[l].sz)];
+      x[q] = v;
+      part += double(v);
+    }
+    const double sum = tail_sum(part, red);
+    const A mean = zm ? A(sum / n) : A(0);
+    for(int q = tid; q < n; q += bd) x[q] -= mean;
+    __syncthreads();
+    tail_sweep<A>(o, B(l), x, S(l), zm, red);
+    tail_sweep<A>(o, B(l), x, S(l), zm, red);
+  }
+  const int n0 = a.lv[0].op.L.count();
+  for(int q = tid; q < n0; q += bd) x_out[q] = X(0)[q];
+  if(tid == 0) {
+    ls_out->sx = 0.0;  // the mean is already removed
+    ls_out->sum_x = 0.0;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // CG kernels (FP64 vectors).
 // ---------------------------------------------------------------------------
 
@@ -900,6 +1157,10 @@ struct PoissonPlan {
   cudaGraphExec_t exec = nullptr;
   long long pre_counts[kKernelCount] = {};
   long long body_counts[kKernelCount] = {};
+  // levels tail_first.. run as one single-block launch (k_vcycle_tail)
+  int tail_first = -1;
+  TailArgs tail{};
+  size_t tail_smem = 0;
 };
 
 namespace {
@@ -983,6 +1244,58 @@ void host_apply(const Grid& g, const PBC& pbc, const std::vector<double>& in,
                               (nb[1][1] - 2.0 * c + nb[1][0]) / (g.dy * g.dy) -
                               (nb[2][1] - 2.0 * c + nb[2][0]) / (g.dz * g.dz);
       }
+}
+
+}  // namespace
+
+namespace {
+
+// Chooses the first level (below the finest) whose cells fit the single-block
+// tail and lays out its shared memory: per level b, x, s (T), then the
+// coarsest solve's FP64 vector.  ORCHARD_B200_NO_TAIL=1 keeps every level on
+// the per-level kernels (for comparisons).
+void setup_tail(PoissonPlan* P, size_t tsz) {
+  const char* e = std::getenv("ORCHARD_B200_NO_TAIL");
+  if(e != nullptr && e[0] == '1') return;
+  const int nl = static_cast<int>(P->levels.size());
+  constexpr size_t kSmemLimit = 200 * 1024;
+  for(int first = 1; first < nl; ++first) {
+    if(P->levels[first].L.count() > kTailMaxCells || nl - first > kTailMaxLevels) continue;
+    TailArgs t{};
+    t.count = nl - first;
+    size_t cursor = 0;  // elements of T
+    const size_t align = 16 / tsz;
+    for(int l = first; l < nl; ++l) {
+      const Level& lv = P->levels[l];
+      TailLevel& tl = t.lv[l - first];
+      tl.op = lv.op;
+      tl.sx = lv.rx == 2 ? 1 : 0;
+      tl.sy = lv.ry == 2 ? 1 : 0;
+      tl.sz = lv.rz == 2 ? 1 : 0;
+      cursor = (cursor + align - 1) / align * align;
+      tl.off = static_cast<int>(cursor);
+      cursor += 3 * static_cast<size_t>(lv.L.count());
+    }
+    cursor = (cursor + align - 1) / align * align;
+    t.coarse_off = static_cast<int>(cursor);
+    t.coarse_n = P->coarse_n;
+    cursor += static_cast<size_t>(P->coarse_n) * sizeof(double) / tsz;
+    const size_t bytes = cursor * tsz;
+    if(bytes > kSmemLimit) continue;
+    t.swaps = P->swaps;
+    t.factors = P->factors;
+    t.zm = P->zero_mean;
+    if(tsz == sizeof(float))
+      OFB_CHECK(cudaFuncSetAttribute(k_vcycle_tail<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(bytes)));
+    else
+      OFB_CHECK(cudaFuncSetAttribute(k_vcycle_tail<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(bytes)));
+    P->tail = t;
+    P->tail_first = first;
+    P->tail_smem = bytes;
+    return;
+  }
 }
 
 }  // namespace
@@ -1101,6 +1414,8 @@ PoissonPlan* poisson_plan_create(const Grid& g, const PBC& pbc_in, int precision
   OFB_CHECK(cudaMemcpy(P->factors, m.data(), static_cast<size_t>(n) * n * sizeof(double),
                        cudaMemcpyHostToDevice));
 
+  setup_tail(P, tsz);
+
   const size_t nf = P->levels[0].L.count();
   OFB_CHECK(cudaMalloc(&P->b, nf * sizeof(double)));
   OFB_CHECK(cudaMalloc(&P->x, nf * sizeof(double)));
@@ -1182,6 +1497,13 @@ void v_cycle(PoissonPlan* P, int l, SolveScalars* sc, RedBuf rb, cudaStream_t s)
   SolveScalars* rz_sc = l == 0 ? sc : nullptr;
   T* a = static_cast<T*>(lv.a);
   T* x = static_cast<T*>(lv.x);
+  if(l == P->tail_first) {
+    ProfScope ps(kKCoarseLevels, s);
+    k_vcycle_tail<T><<<1, kTailThreads, P->tail_smem, s>>>(P->tail, static_cast<const T*>(lv.b),
+                                                           &ls->sb, x, ls);
+    OFB_LAUNCH_CHECK("k_vcycle_tail");
+    return;
+  }
   if(l + 1 == nl) {
     ProfScope ps(kKCoarseSolve, s);
     if(l == 0)
@@ -1200,16 +1522,19 @@ void v_cycle(PoissonPlan* P, int l, SolveScalars* sc, RedBuf rb, cudaStream_t s)
   auto smooth_chain = [&](auto* bptr) {
     using B = std::remove_cv_t<std::remove_pointer_t<decltype(bptr)>>;
     const bool fine = l == 0;
-    {
-      ProfScope ps(fine ? kKSmoothFirstFine : kKCoarseLevels, s);
-      k_smooth_first<T, B><<<ln.grid, ln.block, 0, s>>>(lv.op, bptr, sb_ptr, a, ls, zm, ln.kchunk, rb);
-    }
     const bool vec = vfits<T>(lv.L) && vec_enabled();
     const bool vsm = vec && vec_enabled("smooth");
     const bool vpr = vec && vec_enabled("prolong");
     const bool vre = vec && vec_enabled("restrict");
     const vst::RowLaunch lr = vst::row_launch(lv.L.nx, lv.L.ny, lv.L.nz, vst::Width<T>::W, 16);
-    {
+    if(vsm && vec_enabled("pre")) {
+      ProfScope ps(fine ? kKSmoothFine : kKCoarseLevels, s);
+      k_vsmooth_pre<T, B><<<lr.grid, lr.block, 0, s>>>(lv.op, bptr, sb_ptr, x, ls, zm, lr.kchunk, rb);
+    } else {
+      {
+        ProfScope ps(fine ? kKSmoothFirstFine : kKCoarseLevels, s);
+        k_smooth_first<T, B><<<ln.grid, ln.block, 0, s>>>(lv.op, bptr, sb_ptr, a, ls, zm, ln.kchunk, rb);
+      }
       ProfScope ps(fine ? kKSmoothFine : kKCoarseLevels, s);
       if(vsm)
         k_vsmooth<T, B><<<lr.grid, lr.block, 0, s>>>(lv.op, bptr, sb_ptr, a, &ls->sa, x, ls, zm,

@@ -93,6 +93,10 @@ inline RowLaunch row_launch(int nx, int ny, int nz, int W, int min_chunk) {
   long long cols = static_cast<long long>(gx) * gy;
   int kchunk = min_chunk < nz ? min_chunk : nz;
   if(kchunk < 1) kchunk = 1;
+  // Small levels: shorter chunks, so that enough blocks run at once to hide
+  // the latency of each plane's loads (a long chunk on a few blocks is one
+  // long chain of dependent plane loads).
+  while(kchunk > 1 && cols * ((nz + kchunk - 1) / kchunk) < kTargetBlocks) kchunk /= 2;
   while(cols * ((nz + kchunk - 1) / kchunk) > kMaxBlocks) kchunk *= 2;
   l.kchunk = kchunk;
   l.grid = dim3(gx, gy, (nz + kchunk - 1) / kchunk);
