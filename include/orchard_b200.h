@@ -4,8 +4,7 @@
  * Drop-in boundary for the CPU path of Orchard Flow (zfifteen/solver).  The
  * reference has no FFI layer; its seams are C++ free functions, and each entry
  * point below replaces one of them (cited as file:line in the reference).  The
- * C++ mirror of those functions (solver_b200/host/orchard/...) and the Python
- * binding (solver_b200/_capi.py) are thin layers over this header.
+ * Python binding (solver_b200/_capi.py) is a thin layer over this header.
  *
  * Conventions
  *  - All arrays are the reference's padded MAC storage, double precision,
@@ -217,6 +216,42 @@ of_status of_tg_init(of_ctx* ctx, double viscosity, double dt, int mode);
  * reference throws; the state then holds the last completed step. */
 of_status of_run_steps(of_ctx* ctx, const of_step_params* params, int steps,
                        of_step_metrics* metrics);
+
+/* ---- tangent-linear and adjoint runs -------------------------------------- */
+
+/* No counterpart in the reference: the discrete derivatives of of_run_steps
+ * on periodic grids with the Taylor-Green predictor.  Both start from the
+ * context's resident state and leave it `steps` steps later, as of_run_steps
+ * does.  The advection is linearised with its limiter, upwind and
+ * first-order branches frozen at the base trajectory. */
+
+/* Diagnostics of an adjoint run. */
+typedef struct {
+  double loss;             /* 1/2 |u(T) - target|^2 over the unique velocity entries */
+  double grad_viscosity;   /* d loss / d viscosity */
+  int forward_steps;       /* forward steps run, recomputation included */
+  double forward_ms;       /* device time of the first forward pass */
+  double backward_ms;      /* device time of the recomputation and reverse steps */
+  size_t device_bytes;     /* device memory held by the tangent-linear / adjoint buffers */
+} of_adjoint_info;
+
+/* du, dv, dw (host, padded): a perturbation of the active entries of the
+ * resident velocity.  out_*: the tangent-linear velocity after `steps` steps
+ * (ghosts filled). */
+of_status of_tangent_linear(of_ctx* ctx, const of_step_params* params, int steps, const double* du,
+                            const double* dv, const double* dw, double* out_u, double* out_v,
+                            double* out_w);
+
+/* Gradient of loss = 1/2 sum over the unique velocity entries (the duplicated
+ * periodic face excluded) of (u(T) - target)^2 with respect to the active
+ * entries of the resident velocity (grad_*, host, padded, ghosts zero) and to
+ * the viscosity (info->grad_viscosity).  The state before every
+ * `checkpoint_every` steps is kept; each segment is recomputed from it during
+ * the reverse sweep. */
+of_status of_adjoint_gradient(of_ctx* ctx, const of_step_params* params, int steps,
+                              int checkpoint_every, const double* target_u,
+                              const double* target_v, const double* target_w, double* grad_u,
+                              double* grad_v, double* grad_w, of_adjoint_info* info);
 
 /* ---- allocation-free entry point ---------------------------------------- */
 

@@ -247,6 +247,35 @@ class Context:
         _capi.check(self._lib.of_run_steps(self._h, C.byref(params), int(steps), C.byref(m)))
         return _struct_dict(m)
 
+    # ---- derivatives (periodic grids, Taylor-Green predictor) ----------------
+    def tangent_linear(self, params: _capi.OfStepParams, steps: int, du):
+        """Runs `steps` steps from the resident state and returns the
+        tangent-linear velocity for the perturbation `du` (three padded arrays)
+        of the resident velocity's active entries."""
+        g = self.grid
+        for a, loc in zip(du, "uvw"):
+            _check_shape(g, a, loc, "tangent_linear")
+        out = [g.zeros(c) for c in "uvw"]
+        _capi.check(self._lib.of_tangent_linear(self._h, C.byref(params), int(steps),
+                                                *map(_dp, du), *map(_dp, out)))
+        return out
+
+    def adjoint_gradient(self, params: _capi.OfStepParams, steps: int, target,
+                         checkpoint_every: int = 10):
+        """Runs `steps` steps from the resident state; returns (grad, info) with
+        grad the gradient of 1/2 |u(T) - target|^2 (unique entries) with respect
+        to the resident velocity's active entries and info the loss, the
+        viscosity derivative and the run's timings."""
+        g = self.grid
+        for a, loc in zip(target, "uvw"):
+            _check_shape(g, a, loc, "adjoint_gradient")
+        grad = [g.zeros(c) for c in "uvw"]
+        info = _capi.OfAdjointInfo()
+        _capi.check(self._lib.of_adjoint_gradient(self._h, C.byref(params), int(steps),
+                                                  int(checkpoint_every), *map(_dp, target),
+                                                  *map(_dp, grad), C.byref(info)))
+        return grad, _struct_dict(info)
+
 
 def step_params(viscosity, dt, max_iterations, tolerance, variant=OF_CORRECTION_TAYLOR_GREEN,
                 density=1.0, name=None):

@@ -22,7 +22,8 @@ EXPORTED_SYMBOLS = (
     "of_device_bytes", "of_compute_advection_term", "of_solve_predictor_adi",
     "of_solve_pressure_poisson", "of_project_velocity", "of_state_upload", "of_state_download",
     "of_tg_init", "of_run_steps", "of_stream", "of_kernel_class_count", "of_kernel_class_name",
-    "of_profile_enable", "of_profile_reset", "of_profile_read",
+    "of_profile_enable", "of_profile_reset", "of_profile_read", "of_tangent_linear",
+    "of_adjoint_gradient", "of_pressure_rhs_noalloc",
 )
 
 
@@ -77,6 +78,12 @@ class OfStepParams(C.Structure):
                 ("solver_name", C.c_char_p)]
 
 
+class OfAdjointInfo(C.Structure):
+    _fields_ = [("loss", C.c_double), ("grad_viscosity", C.c_double), ("forward_steps", C.c_int),
+                ("forward_ms", C.c_double), ("backward_ms", C.c_double),
+                ("device_bytes", C.c_size_t)]
+
+
 DP = C.POINTER(C.c_double)
 
 _lib = None
@@ -112,6 +119,9 @@ def load():
         # device pointers (u, v, w, pressure_rhs, stream) as c_void_p
         lib.of_pressure_rhs_noalloc.argtypes = [C.POINTER(OfGrid), C.c_double, C.c_double] + \
             [C.c_void_p] * 4 + [DP, C.c_void_p]
+        lib.of_tangent_linear.argtypes = [C.c_void_p, C.POINTER(OfStepParams), C.c_int] + [DP] * 6
+        lib.of_adjoint_gradient.argtypes = [C.c_void_p, C.POINTER(OfStepParams), C.c_int,
+                                            C.c_int] + [DP] * 6 + [C.POINTER(OfAdjointInfo)]
         lib.of_kernel_class_name.restype = C.c_char_p
         lib.of_profile_enable.argtypes = [C.c_int]
         lib.of_profile_read.argtypes = [C.c_int, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),

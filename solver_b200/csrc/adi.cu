@@ -254,6 +254,11 @@ int adi_line_count(const AdiPlan* p, int comp, int axis) {
 
 bool adi_axis_active(const AdiPlan* p, int comp, int axis) { return p->ax[comp][axis].active; }
 
+void adi_axis_geometry(const AdiPlan* p, int comp, int axis, int* begin, int* n) {
+  *begin = p->ax[comp][axis].begin;
+  *n = p->ax[comp][axis].n;
+}
+
 namespace {
 
 struct SweepArgs {

@@ -5,6 +5,7 @@
 #include "../../include/orchard_b200.h"
 #include "kernels.hpp"
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -55,6 +56,49 @@ using ofb::Lay;
 using ofb::PBC;
 using ofb::VBC;
 
+namespace {
+
+// Device buffers of the tangent-linear and adjoint runs, allocated on first
+// use and kept with the context.
+struct SavedState {
+  double* vel[3] = {nullptr, nullptr, nullptr};
+  double* adv_prev[3] = {nullptr, nullptr, nullptr};
+  double* p = nullptr;
+  int has_prev = 0;
+  bool clean = false;
+};
+
+struct AdjWork {
+  std::vector<double*> owned;
+  size_t bytes = 0;
+  int steps = 0, every = 0;
+  // tangent-linear state and the base velocity it is linearised about
+  double *t_vel[3], *t_adv_prev[3], *t_adv_cur[3], *t_corr[3], *t_p, *base_cur[3];
+  // adjoint variables
+  double *lam_vel[3], *lam_corr[3], *lam_pred[3], *lam_b[3], *lam_cur[3], *lam_prev[3],
+      *lam_advtot[3], *target[3], *out[3];
+  double *lam_p, *lam_phi, *lam_q;
+  // recomputed intermediates of the step being differentiated
+  double *y[3][3], *rc_adv[3], *rc_corr[3];
+  // working state of a segment recomputation
+  double *w_vel[3], *w_adv_prev[3], *w_adv_cur[3], *w_corr[3], *w_p;
+  std::vector<SavedState> ckpt, seg;
+  double* acc = nullptr;  // [0] loss, [1] d/dnu (direct), [2] sum mu.D y of the sweeps
+  ~AdjWork() {
+    for(double* p : owned) cudaFree(p);
+  }
+  double* alloc(size_t n, cudaStream_t s) {
+    double* p = nullptr;
+    OFB_CHECK(cudaMalloc(&p, n * sizeof(double)));
+    OFB_CHECK(cudaMemsetAsync(p, 0, n * sizeof(double), s));
+    owned.push_back(p);
+    bytes += n * sizeof(double);
+    return p;
+  }
+};
+
+}  // namespace
+
 struct of_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -90,10 +134,12 @@ struct of_ctx {
   ofb::AdiPlan* adi = nullptr;
   double adi_alpha = -1.0;
   size_t bytes = 0;
+  AdjWork* adj = nullptr;
 
   ~of_ctx() {
     cudaSetDevice(device);
     if(stream) cudaStreamSynchronize(stream);
+    delete adj;
     for(int c = 0; c < 3; ++c) {
       cudaFree(vel[c]);
       cudaFree(adv_prev[c]);
@@ -242,8 +288,12 @@ ofb::SolveScalars run_poisson(of_ctx* ctx, int max_iterations, double tolerance,
 }
 
 // solve_predictor_adi on the context's rhs buffers; returns pointers to the
-// three predicted components (rhs[] or adi_b[]).
-void predictor_adi(of_ctx* ctx, double alpha, double* out[3], int* line_solves) {
+// three predicted components (rhs[] or adi_b[]).  With sweep_out, sweep
+// (component, axis) writes into sweep_out[component][axis] instead of the
+// ping-pong buffers, so every sweep's output survives the call (the adjoint
+// needs them for the viscosity derivative).
+void predictor_adi(of_ctx* ctx, double alpha, double* out[3], int* line_solves,
+                   double* const (*sweep_out)[3] = nullptr) {
   ofb::AdiPlan* plan = alpha != 0.0 ? ctx->adi_for(alpha) : nullptr;
   int lines = 0;
   for(int c = 0; c < 3; ++c) {
@@ -256,15 +306,356 @@ void predictor_adi(of_ctx* ctx, double alpha, double* out[3], int* line_solves) 
     }
     for(int axis = 0; axis < 3; ++axis) {
       if(ofb::adi_axis_active(plan, c, axis)) {
-        ofb::launch_adi_sweep(plan, c, axis, a, b, ctx->stream);
+        if(sweep_out != nullptr) {
+          ofb::launch_adi_sweep(plan, c, axis, a, sweep_out[c][axis], ctx->stream);
+          a = sweep_out[c][axis];
+        } else {
+          ofb::launch_adi_sweep(plan, c, axis, a, b, ctx->stream);
+          std::swap(a, b);
+        }
         lines += ofb::adi_line_count(plan, c, axis);
-        std::swap(a, b);
       }
       ofb::launch_component_bc(ctx->g, ctx->bc, c, a, ctx->stream);
     }
     out[c] = a;
   }
   if(line_solves) *line_solves = lines;
+}
+
+// A time-step state: velocity, AB2 advection history, total pressure, and the
+// velocity buffer the step writes before the buffers are exchanged.  The
+// context's resident state is one; the tangent-linear run keeps another.
+struct StepState {
+  double* vel[3];
+  double* adv_prev[3];
+  double* adv_cur[3];
+  double* p;
+  double* corrected[3];
+  int has_prev;
+  bool clean;  // velocity ghosts already filled
+};
+
+StepState resident_state(of_ctx* ctx) {
+  StepState st{};
+  for(int c = 0; c < 3; ++c) {
+    st.vel[c] = ctx->vel[c];
+    st.adv_prev[c] = ctx->adv_prev[c];
+    st.adv_cur[c] = ctx->adv_cur[c];
+    st.corrected[c] = ctx->corrected[c];
+  }
+  st.p = ctx->p_total;
+  st.has_prev = ctx->has_prev;
+  st.clean = ctx->state_clean;
+  return st;
+}
+
+void set_resident_state(of_ctx* ctx, const StepState& st) {
+  for(int c = 0; c < 3; ++c) {
+    ctx->vel[c] = st.vel[c];
+    ctx->adv_prev[c] = st.adv_prev[c];
+    ctx->adv_cur[c] = st.adv_cur[c];
+    ctx->corrected[c] = st.corrected[c];
+  }
+  ctx->p_total = st.p;
+  ctx->has_prev = st.has_prev;
+  ctx->state_clean = st.clean;
+}
+
+// Options of one step for the adjoint machinery.
+struct StepHooks {
+  // tangent-linear step: the advection is linearised about these velocities
+  // (the base trajectory's current velocity) and applied to the state's
+  const double* const* lin_base = nullptr;
+  // when set, every ADI sweep output is kept (predictor_adi's sweep_out)
+  double* const (*sweep_out)[3] = nullptr;
+  // stop after the pressure rhs (ctx->prhs) is formed: no solve, no update
+  bool stop_after_rhs = false;
+};
+
+// One projection step on `st` (the loop body of run_taylor_green_steps,
+// solver/taylor_green.cpp:577-633, and of advance_lid_driven_cavity_impl,
+// solver/lid_driven_cavity.cpp:562-623).  Returns the step's diagnostics.
+ofb::SolveScalars forward_step(of_ctx* ctx, const of_step_params* prm, const std::string& name,
+                               int step_no, StepState& st, const StepHooks* hk = nullptr) {
+  const double dt = prm->dt;
+  const double nu = prm->viscosity;
+  const double alpha = 0.5 * nu * dt;
+  ofb::PoissonPlan* plan = ctx->poisson_for(ctx->pbc);
+  cudaStream_t s = ctx->stream;
+  const Grid& g = ctx->g;
+  // current = state.velocity with boundary conditions (solver/taylor_green.cpp:578-579)
+  const double* cur[3] = {st.vel[0], st.vel[1], st.vel[2]};
+  if(!st.clean) {
+    for(int c = 0; c < 3; ++c) ctx->d2d(st.corrected[c], st.vel[c], 1 + c);
+    ofb::launch_velocity_bc(g, ctx->bc, st.corrected[0], st.corrected[1], st.corrected[2], s);
+    for(int c = 0; c < 3; ++c) cur[c] = st.corrected[c];
+  }
+  // assemble_predictor_rhs (fused)
+  ofb::PredictorArgs pa{};
+  pa.g = g;
+  for(int c = 0; c < 3; ++c) {
+    pa.cur[c] = cur[c];
+    pa.prev[c] = st.adv_prev[c];
+    pa.adv[c] = st.adv_cur[c];
+    pa.rhs[c] = ctx->rhs[c];
+  }
+  pa.p = st.p;
+  pa.nu = nu;
+  pa.dt = dt;
+  pa.alpha = alpha;
+  pa.has_prev = st.has_prev;
+  pa.variant = prm->correction_variant;
+  if(hk != nullptr && hk->lin_base != nullptr) {
+    ofb::launch_advection_jvp(g, hk->lin_base, cur, st.adv_cur, s);
+    ofb::launch_predictor_rest(pa, s);
+  } else {
+    ofb::launch_predictor_rhs(pa, s);
+  }
+  // solve_predictor_adi
+  double* pred[3];
+  predictor_adi(ctx, alpha, pred, nullptr, hk != nullptr ? hk->sweep_out : nullptr);
+  // project_velocity with a zero initial pressure correction
+  ofb::launch_divergence_rhs(g, ctx->pbc, pred[0], pred[1], pred[2], prm->density / dt, ctx->prhs,
+                             ofb::poisson_b(plan), ctx->sc, ctx->rb, s);
+  if(hk != nullptr && hk->stop_after_rhs) return ofb::SolveScalars{};
+  // pressure_correction.fill(0.0) (solver/taylor_green.cpp:596): x = 0, mean 0
+  OFB_CHECK(cudaMemsetAsync(ofb::poisson_x(plan), 0, sizeof(double) * g.nx * g.ny * g.nz, s));
+  OFB_CHECK(cudaMemsetAsync(&ctx->sc->sx, 0, sizeof(double), s));
+  const ofb::SolveScalars ps =
+      run_poisson(ctx, prm->poisson_max_iterations, prm->poisson_tolerance, nullptr, 0);
+  if(!ps.converged) {
+    std::ostringstream m;
+    m << name << " pressure solve did not converge at step " << step_no
+      << " (iterations=" << ps.iterations << ", relative_residual=" << ps.rel
+      << ", tolerance=" << prm->poisson_tolerance << ")";
+    fail(OF_NOT_CONVERGED, m.str());
+  }
+  ofb::launch_correct_velocity(g, ctx->pbc, ofb::poisson_x(plan), ctx->sc, pred[0], pred[1],
+                               pred[2], -dt / prm->density, st.corrected[0], st.corrected[1],
+                               st.corrected[2], st.vel[0], st.vel[1], st.vel[2], ctx->sc,
+                               ctx->rb, s);
+  ofb::launch_velocity_bc(g, ctx->bc, st.corrected[0], st.corrected[1], st.corrected[2], s);
+  ofb::CellPassArgs cp{};
+  cp.g = g;
+  cp.u = st.corrected[0];
+  cp.v = st.corrected[1];
+  cp.w = st.corrected[2];
+  cp.x = ofb::poisson_x(plan);
+  cp.p_total = st.p;
+  cp.rhs_padded = ctx->prhs;
+  cp.p_rhs_scale = -0.5 * nu * dt;
+  cp.dt = dt;
+  ofb::launch_cell_pass(cp, ctx->sc, ctx->rb, s);
+  ofb::launch_total_pressure_bc(g, ctx->bc, nu, st.corrected[0], st.corrected[1],
+                                st.corrected[2], st.p, s);
+  OFB_CHECK(cudaMemcpyAsync(ctx->sc_host, ctx->sc, sizeof(ofb::SolveScalars),
+                            cudaMemcpyDeviceToHost, s));
+  ctx->sync();
+  const ofb::SolveScalars d = *ctx->sc_host;
+  if(d.nonfinite) fail(OF_NONFINITE, name + " solve produced a non-finite state");
+  for(int c = 0; c < 3; ++c) {
+    std::swap(st.vel[c], st.corrected[c]);
+    std::swap(st.adv_prev[c], st.adv_cur[c]);
+  }
+  st.has_prev = 1;
+  st.clean = true;
+  return d;
+}
+
+// ---------------------------------------------------------------------------
+// Tangent-linear and adjoint runs (periodic grids, Taylor-Green predictor).
+// ---------------------------------------------------------------------------
+
+AdjWork* adj_work(of_ctx* ctx, int steps, int every) {
+  AdjWork* W = ctx->adj;
+  const int nseg = (steps + every - 1) / every;
+  if(W != nullptr && W->steps == steps && W->every == every) return W;
+  ctx->sync();
+  delete W;
+  ctx->adj = nullptr;
+  W = new AdjWork();
+  cudaStream_t s = ctx->stream;
+  auto face = [&](int c) { return ctx->size(1 + c); };
+  const size_t cell = ctx->size(0);
+  for(int c = 0; c < 3; ++c) {
+    for(double** b : {&W->t_vel[c], &W->t_adv_prev[c], &W->t_adv_cur[c], &W->t_corr[c], &W->base_cur[c],
+                      &W->lam_vel[c], &W->lam_corr[c], &W->lam_pred[c], &W->lam_b[c], &W->lam_cur[c],
+                      &W->lam_prev[c], &W->lam_advtot[c], &W->target[c], &W->out[c], &W->rc_adv[c],
+                      &W->rc_corr[c], &W->w_vel[c], &W->w_adv_prev[c], &W->w_adv_cur[c], &W->w_corr[c]})
+      *b = W->alloc(face(c), s);
+    for(int a = 0; a < 3; ++a) W->y[c][a] = W->alloc(face(c), s);
+  }
+  W->t_p = W->alloc(cell, s);
+  W->w_p = W->alloc(cell, s);
+  W->lam_p = W->alloc(cell, s);
+  W->lam_phi = W->alloc(cell, s);
+  W->lam_q = W->alloc(cell, s);
+  W->acc = W->alloc(4, s);
+  auto saved = [&]() {
+    SavedState t;
+    for(int c = 0; c < 3; ++c) {
+      t.vel[c] = W->alloc(face(c), s);
+      t.adv_prev[c] = W->alloc(face(c), s);
+    }
+    t.p = W->alloc(cell, s);
+    return t;
+  };
+  for(int k = 0; k < nseg; ++k) W->ckpt.push_back(saved());
+  for(int k = 0; k < every && k < steps; ++k) W->seg.push_back(saved());
+  W->steps = steps;
+  W->every = every;
+  ctx->adj = W;
+  return W;
+}
+
+// The base-trajectory velocity buffers of the work set take the resident
+// velocity's edge and corner ghosts (constants of every step), as the
+// context's own velocity buffers do.
+void adopt_edges(of_ctx* ctx, AdjWork* W) {
+  for(int c = 0; c < 3; ++c)
+    for(double* b : {W->w_vel[c], W->w_corr[c], W->rc_corr[c], W->base_cur[c]})
+      ctx->d2d(b, ctx->vel[c], 1 + c);
+}
+
+void save_state(of_ctx* ctx, const StepState& st, SavedState& out) {
+  for(int c = 0; c < 3; ++c) {
+    ctx->d2d(out.vel[c], st.vel[c], 1 + c);
+    ctx->d2d(out.adv_prev[c], st.adv_prev[c], 1 + c);
+  }
+  ctx->d2d(out.p, st.p, 0);
+  out.has_prev = st.has_prev;
+  out.clean = st.clean;
+}
+
+void load_state(of_ctx* ctx, const SavedState& in, StepState& st) {
+  for(int c = 0; c < 3; ++c) {
+    ctx->d2d(st.vel[c], in.vel[c], 1 + c);
+    ctx->d2d(st.adv_prev[c], in.adv_prev[c], 1 + c);
+  }
+  ctx->d2d(st.p, in.p, 0);
+  st.has_prev = in.has_prev;
+  st.clean = in.clean;
+}
+
+void require_adjoint_case(of_ctx* ctx, const of_step_params* prm) {
+  for(int f = 0; f < 6; ++f)
+    if(ctx->bc.type[f] != ofb::kPeriodic)
+      fail(OF_INVALID_ARGUMENT, "the tangent-linear and adjoint runs support periodic boundaries only");
+  if(prm->correction_variant != OF_CORRECTION_TAYLOR_GREEN)
+    fail(OF_INVALID_ARGUMENT, "the tangent-linear and adjoint runs support the Taylor-Green predictor only");
+}
+
+void zero(of_ctx* ctx, double* p, int loc) {
+  OFB_CHECK(cudaMemsetAsync(p, 0, ctx->size(loc) * sizeof(double), ctx->stream));
+}
+
+// The velocity the step at state `st` advects: the state's own buffers when
+// clean, else a ghost-filled copy in `scratch`.
+void current_velocity(of_ctx* ctx, const StepState& st, double* const* scratch, const double* cur[3]) {
+  if(st.clean) {
+    for(int c = 0; c < 3; ++c) cur[c] = st.vel[c];
+    return;
+  }
+  for(int c = 0; c < 3; ++c) ctx->d2d(scratch[c], st.vel[c], 1 + c);
+  ofb::launch_velocity_bc(ctx->g, ctx->bc, scratch[0], scratch[1], scratch[2], ctx->stream);
+  for(int c = 0; c < 3; ++c) cur[c] = scratch[c];
+}
+
+// Reverse step: given the adjoints of the step's outputs (W->lam_vel, the
+// AB2 history W->lam_prev, the total pressure W->lam_p), forms those of its
+// inputs in the same buffers.  `S` is the state the step started from.
+void adjoint_step(of_ctx* ctx, const of_step_params* prm, AdjWork* W, const SavedState& S) {
+  const Grid& g = ctx->g;
+  cudaStream_t s = ctx->stream;
+  const double dt = prm->dt, nu = prm->viscosity, rho = prm->density;
+  const double alpha = 0.5 * nu * dt;
+  ofb::PoissonPlan* plan = ctx->poisson_for(ctx->pbc);
+  // recompute the step's predictor, sweeps and pressure rhs from S
+  StepState rs{};
+  for(int c = 0; c < 3; ++c) {
+    rs.vel[c] = S.vel[c];
+    rs.adv_prev[c] = S.adv_prev[c];
+    rs.adv_cur[c] = W->rc_adv[c];
+    rs.corrected[c] = W->rc_corr[c];
+  }
+  rs.p = S.p;
+  rs.has_prev = S.has_prev;
+  rs.clean = S.clean;
+  StepHooks hk;
+  hk.sweep_out = W->y;
+  hk.stop_after_rhs = true;
+  forward_step(ctx, prm, "adjoint", 0, rs, &hk);
+  const double* cur[3];
+  for(int c = 0; c < 3; ++c) cur[c] = S.clean ? S.vel[c] : W->rc_corr[c];
+  // total pressure: ghost fill, then p += phi - 0.5 nu dt q
+  ofb::launch_pressure_bc_T(g, W->lam_p, s);
+  zero(ctx, W->lam_phi, 0);
+  zero(ctx, W->lam_q, 0);
+  ofb::launch_axpby_active(g, ofb::kCell, 1.0, W->lam_p, 0.0, nullptr, W->lam_phi, s);
+  ofb::launch_axpby_active(g, ofb::kCell, -0.5 * nu * dt, W->lam_p, 0.0, nullptr, W->lam_q, s);
+  ofb::launch_dot_active(g, ofb::kCell, W->lam_p, ctx->prhs, -0.5 * dt, W->acc + 1, ctx->rb, s);
+  // velocity ghost fill and correction u = u* - (dt/rho) G phi
+  for(int c = 0; c < 3; ++c) {
+    ctx->d2d(W->lam_corr[c], W->lam_vel[c], 1 + c);
+    zero(ctx, W->lam_pred[c], 1 + c);
+  }
+  ofb::launch_velocity_bc_T(g, W->lam_corr[0], W->lam_corr[1], W->lam_corr[2], s);
+  for(int c = 0; c < 3; ++c)
+    ofb::launch_axpby_active(g, ofb::kFaceX + c, 1.0, W->lam_corr[c], 0.0, nullptr, W->lam_pred[c], s);
+  ofb::launch_correct_T(g, -dt / rho, W->lam_corr, W->lam_phi, s);
+  // pressure solve: phi = M q with M symmetric, so lam_q += M lam_phi
+  ofb::launch_rhs_to_system(g, ctx->pbc, W->lam_phi, ofb::poisson_b(plan), ctx->sc, ctx->rb, s);
+  OFB_CHECK(cudaMemsetAsync(ofb::poisson_x(plan), 0, sizeof(double) * g.nx * g.ny * g.nz, s));
+  OFB_CHECK(cudaMemsetAsync(&ctx->sc->sx, 0, sizeof(double), s));
+  const ofb::SolveScalars ps =
+      run_poisson(ctx, prm->poisson_max_iterations, prm->poisson_tolerance, nullptr, 0);
+  if(!ps.converged && ps.r0 > 0.0) {
+    std::ostringstream m;
+    m << "adjoint pressure solve did not converge (iterations=" << ps.iterations
+      << ", relative_residual=" << ps.rel << ")";
+    fail(OF_NOT_CONVERGED, m.str());
+  }
+  ofb::launch_add_compact(g, ofb::poisson_x(plan), ctx->sc, W->lam_q, s);
+  // divergence q = (rho/dt) D u*
+  ofb::launch_divergence_T(g, rho / dt, W->lam_q, W->lam_pred, s);
+  // ADI: BC(rhs), then per axis sweep + BC, undone in reverse
+  ofb::AdiPlan* adi = ctx->adi_for(alpha);
+  double* lam_rhs[3];
+  for(int c = 0; c < 3; ++c) {
+    double* a = W->lam_pred[c];
+    double* b = W->lam_b[c];
+    for(int axis = 2; axis >= 0; --axis) {
+      ofb::launch_component_bc_T(g, c, a, s);
+      if(!ofb::adi_axis_active(adi, c, axis)) continue;
+      const bool dup = axis == c;  // periodic normal component: duplicated face
+      if(dup) ofb::launch_duplicate(g, c, true, a, s);
+      zero(ctx, b, 1 + c);
+      ofb::launch_adi_sweep(adi, c, axis, a, b, s);
+      if(dup) ofb::launch_duplicate(g, c, false, b, s);
+      int begin = 0, n = 0;
+      ofb::adi_axis_geometry(adi, c, axis, &begin, &n);
+      ofb::launch_adi_alpha_dot(g, c, axis, begin, n, b, W->y[c][axis], W->acc + 2, ctx->rb, s);
+      std::swap(a, b);
+    }
+    ofb::launch_component_bc_T(g, c, a, s);
+    lam_rhs[c] = a;
+    W->lam_b[c] = b;
+    W->lam_pred[c] = a;
+  }
+  // predictor rhs: 27-point operator, pressure gradient, AB2 combination
+  for(int c = 0; c < 3; ++c) zero(ctx, W->lam_cur[c], 1 + c);
+  ofb::launch_predictor_T(g, nu, dt, alpha, lam_rhs, W->lam_cur, W->lam_p, s);
+  const double s_adv = S.has_prev ? -1.5 * dt : -dt;
+  for(int c = 0; c < 3; ++c) {
+    ofb::launch_axpby_active(g, ofb::kFaceX + c, s_adv, lam_rhs[c], 1.0, W->lam_prev[c],
+                             W->lam_advtot[c], s);
+    ofb::launch_axpby_active(g, ofb::kFaceX + c, S.has_prev ? 0.5 * dt : 0.0, lam_rhs[c], 0.0,
+                             nullptr, W->lam_prev[c], s);
+  }
+  ofb::launch_predictor_nu_dot(g, dt, alpha, cur, lam_rhs, W->acc + 1, ctx->rb, s);
+  ofb::launch_advection_vjp(g, cur, W->lam_advtot, W->lam_cur, s);
+  if(!S.clean) ofb::launch_velocity_bc_T(g, W->lam_cur[0], W->lam_cur[1], W->lam_cur[2], s);
+  for(int c = 0; c < 3; ++c) std::swap(W->lam_vel[c], W->lam_cur[c]);
 }
 
 }  // namespace
@@ -590,82 +981,16 @@ of_status of_run_steps(of_ctx* ctx, const of_step_params* prm, int steps, of_ste
       fail(OF_INVALID_ARGUMENT, "solve_pressure_poisson expects tolerance > 0");
     const std::string name = prm->solver_name ? prm->solver_name : "Taylor-Green";
     const double dt = prm->dt;
-    const double nu = prm->viscosity;
-    const double alpha = 0.5 * nu * dt;
-    ofb::PoissonPlan* plan = ctx->poisson_for(ctx->pbc);
-    cudaStream_t s = ctx->stream;
-    const Grid& g = ctx->g;
     for(int step = 0; step < steps; ++step) {
-      // current = state.velocity with boundary conditions (solver/taylor_green.cpp:578-579)
-      const double* cur[3] = {ctx->vel[0], ctx->vel[1], ctx->vel[2]};
-      if(!ctx->state_clean) {
-        for(int c = 0; c < 3; ++c) ctx->d2d(ctx->corrected[c], ctx->vel[c], 1 + c);
-        ofb::launch_velocity_bc(g, ctx->bc, ctx->corrected[0], ctx->corrected[1], ctx->corrected[2], s);
-        for(int c = 0; c < 3; ++c) cur[c] = ctx->corrected[c];
+      StepState st = resident_state(ctx);
+      ofb::SolveScalars d;
+      try {
+        d = forward_step(ctx, prm, name, ctx->metrics.step + 1, st);
+      } catch(...) {
+        set_resident_state(ctx, st);
+        throw;
       }
-      // assemble_predictor_rhs (fused)
-      ofb::PredictorArgs pa{};
-      pa.g = g;
-      for(int c = 0; c < 3; ++c) {
-        pa.cur[c] = cur[c];
-        pa.prev[c] = ctx->adv_prev[c];
-        pa.adv[c] = ctx->adv_cur[c];
-        pa.rhs[c] = ctx->rhs[c];
-      }
-      pa.p = ctx->p_total;
-      pa.nu = nu;
-      pa.dt = dt;
-      pa.alpha = alpha;
-      pa.has_prev = ctx->has_prev;
-      pa.variant = prm->correction_variant;
-      ofb::launch_predictor_rhs(pa, s);
-      // solve_predictor_adi
-      double* pred[3];
-      predictor_adi(ctx, alpha, pred, nullptr);
-      // project_velocity with a zero initial pressure correction
-      ofb::launch_divergence_rhs(g, ctx->pbc, pred[0], pred[1], pred[2], prm->density / dt, ctx->prhs,
-                                 ofb::poisson_b(plan), ctx->sc, ctx->rb, s);
-      // pressure_correction.fill(0.0) (solver/taylor_green.cpp:596): x = 0, mean 0
-      OFB_CHECK(cudaMemsetAsync(ofb::poisson_x(plan), 0, sizeof(double) * g.nx * g.ny * g.nz, s));
-      OFB_CHECK(cudaMemsetAsync(&ctx->sc->sx, 0, sizeof(double), s));
-      const ofb::SolveScalars ps =
-          run_poisson(ctx, prm->poisson_max_iterations, prm->poisson_tolerance, nullptr, 0);
-      if(!ps.converged) {
-        std::ostringstream m;
-        m << name << " pressure solve did not converge at step " << (step + 1)
-          << " (iterations=" << ps.iterations << ", relative_residual=" << ps.rel
-          << ", tolerance=" << prm->poisson_tolerance << ")";
-        fail(OF_NOT_CONVERGED, m.str());
-      }
-      ofb::launch_correct_velocity(g, ctx->pbc, ofb::poisson_x(plan), ctx->sc, pred[0], pred[1],
-                                   pred[2], -dt / prm->density, ctx->corrected[0], ctx->corrected[1],
-                                   ctx->corrected[2], ctx->vel[0], ctx->vel[1], ctx->vel[2], ctx->sc,
-                                   ctx->rb, s);
-      ofb::launch_velocity_bc(g, ctx->bc, ctx->corrected[0], ctx->corrected[1], ctx->corrected[2], s);
-      ofb::CellPassArgs cp{};
-      cp.g = g;
-      cp.u = ctx->corrected[0];
-      cp.v = ctx->corrected[1];
-      cp.w = ctx->corrected[2];
-      cp.x = ofb::poisson_x(plan);
-      cp.p_total = ctx->p_total;
-      cp.rhs_padded = ctx->prhs;
-      cp.p_rhs_scale = -0.5 * nu * dt;
-      cp.dt = dt;
-      ofb::launch_cell_pass(cp, ctx->sc, ctx->rb, s);
-      ofb::launch_total_pressure_bc(g, ctx->bc, nu, ctx->corrected[0], ctx->corrected[1],
-                                    ctx->corrected[2], ctx->p_total, s);
-      OFB_CHECK(cudaMemcpyAsync(ctx->sc_host, ctx->sc, sizeof(ofb::SolveScalars),
-                                cudaMemcpyDeviceToHost, s));
-      ctx->sync();
-      const ofb::SolveScalars d = *ctx->sc_host;
-      if(d.nonfinite) fail(OF_NONFINITE, name + " solve produced a non-finite state");
-      for(int c = 0; c < 3; ++c) {
-        std::swap(ctx->vel[c], ctx->corrected[c]);
-        std::swap(ctx->adv_prev[c], ctx->adv_cur[c]);
-      }
-      ctx->has_prev = 1;
-      ctx->state_clean = true;
+      set_resident_state(ctx, st);
       of_step_metrics& m = ctx->metrics;
       m.step += 1;
       m.time += dt;
@@ -679,6 +1004,189 @@ of_status of_run_steps(of_ctx* ctx, const of_step_params* prm, int steps, of_ste
       m.pressure_relative_residual = d.rel;
     }
     if(out) *out = ctx->metrics;
+  });
+}
+
+of_status of_tangent_linear(of_ctx* ctx, const of_step_params* prm, int steps, const double* du,
+                            const double* dv, const double* dw, double* out_u, double* out_v,
+                            double* out_w) {
+  return guarded([&] {
+    require_ctx(ctx);
+    require_ptr(prm, "step parameters");
+    const double* din[3] = {du, dv, dw};
+    double* dout[3] = {out_u, out_v, out_w};
+    for(int c = 0; c < 3; ++c) {
+      require_ptr(din[c], "velocity perturbation");
+      require_ptr(dout[c], "tangent-linear output");
+    }
+    if(steps < 1) fail(OF_INVALID_ARGUMENT, "the tangent-linear run needs at least one step");
+    require_adjoint_case(ctx, prm);
+    const std::string name = prm->solver_name ? prm->solver_name : "Taylor-Green";
+    AdjWork* W = adj_work(ctx, steps, steps);
+    StepState st = resident_state(ctx);
+    adopt_edges(ctx, W);
+    StepState t{};
+    for(int c = 0; c < 3; ++c) {
+      t.vel[c] = W->t_vel[c];
+      t.adv_prev[c] = W->t_adv_prev[c];
+      t.adv_cur[c] = W->t_adv_cur[c];
+      t.corrected[c] = W->t_corr[c];
+      // only the active entries of the perturbation count (ghosts are refilled,
+      // edges are constants of the step)
+      ctx->upload(W->out[c], din[c], 1 + c);
+      zero(ctx, t.vel[c], 1 + c);
+      ofb::launch_axpby_active(ctx->g, ofb::kFaceX + c, 1.0, W->out[c], 0.0, nullptr, t.vel[c],
+                               ctx->stream);
+      zero(ctx, t.adv_prev[c], 1 + c);
+      zero(ctx, t.adv_cur[c], 1 + c);
+      zero(ctx, t.corrected[c], 1 + c);
+    }
+    t.p = W->t_p;
+    zero(ctx, t.p, 0);
+    t.has_prev = st.has_prev;
+    t.clean = false;
+    try {
+      for(int n = 0; n < steps; ++n) {
+        const double* base[3];
+        current_velocity(ctx, st, W->base_cur, base);
+        StepHooks hk;
+        hk.lin_base = base;
+        forward_step(ctx, prm, name + " tangent-linear", n + 1, t, &hk);
+        forward_step(ctx, prm, name, ctx->metrics.step + 1, st);
+        ctx->metrics.step += 1;
+        ctx->metrics.time += prm->dt;
+      }
+    } catch(...) {
+      set_resident_state(ctx, st);
+      for(int c = 0; c < 3; ++c) {
+        W->t_vel[c] = t.vel[c];
+        W->t_adv_prev[c] = t.adv_prev[c];
+        W->t_adv_cur[c] = t.adv_cur[c];
+        W->t_corr[c] = t.corrected[c];
+      }
+      throw;
+    }
+    set_resident_state(ctx, st);
+    for(int c = 0; c < 3; ++c) {
+      W->t_vel[c] = t.vel[c];
+      W->t_adv_prev[c] = t.adv_prev[c];
+      W->t_adv_cur[c] = t.adv_cur[c];
+      W->t_corr[c] = t.corrected[c];
+      ctx->download(dout[c], t.vel[c], 1 + c);
+    }
+    ctx->sync();
+  });
+}
+
+of_status of_adjoint_gradient(of_ctx* ctx, const of_step_params* prm, int steps,
+                              int checkpoint_every, const double* target_u,
+                              const double* target_v, const double* target_w, double* grad_u,
+                              double* grad_v, double* grad_w, of_adjoint_info* info) {
+  return guarded([&] {
+    require_ctx(ctx);
+    require_ptr(prm, "step parameters");
+    const double* tin[3] = {target_u, target_v, target_w};
+    double* gout[3] = {grad_u, grad_v, grad_w};
+    for(int c = 0; c < 3; ++c) {
+      require_ptr(tin[c], "target velocity");
+      require_ptr(gout[c], "gradient output");
+    }
+    if(steps < 1) fail(OF_INVALID_ARGUMENT, "the adjoint run needs at least one step");
+    if(checkpoint_every < 1) fail(OF_INVALID_ARGUMENT, "checkpoint_every must be positive");
+    require_adjoint_case(ctx, prm);
+    const std::string name = prm->solver_name ? prm->solver_name : "Taylor-Green";
+    const int every = checkpoint_every < steps ? checkpoint_every : steps;
+    AdjWork* W = adj_work(ctx, steps, every);
+    adopt_edges(ctx, W);
+    const Grid& g = ctx->g;
+    cudaStream_t s = ctx->stream;
+    cudaEvent_t e0, e1, e2;
+    OFB_CHECK(cudaEventCreate(&e0));
+    OFB_CHECK(cudaEventCreate(&e1));
+    OFB_CHECK(cudaEventCreate(&e2));
+    struct EventGuard {
+      cudaEvent_t a, b, c;
+      ~EventGuard() {
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        cudaEventDestroy(c);
+      }
+    } guard{e0, e1, e2};
+    for(int c = 0; c < 3; ++c) ctx->upload(W->target[c], tin[c], 1 + c);
+    OFB_CHECK(cudaMemsetAsync(W->acc, 0, 4 * sizeof(double), s));
+    int forward_steps = 0;
+    // forward run, keeping the state before every segment of `every` steps
+    OFB_CHECK(cudaEventRecord(e0, s));
+    StepState st = resident_state(ctx);
+    try {
+      for(int n = 0; n < steps; ++n) {
+        if(n % every == 0) save_state(ctx, st, W->ckpt[n / every]);
+        forward_step(ctx, prm, name, ctx->metrics.step + 1, st);
+        ctx->metrics.step += 1;
+        ctx->metrics.time += prm->dt;
+        ++forward_steps;
+      }
+    } catch(...) {
+      set_resident_state(ctx, st);
+      throw;
+    }
+    set_resident_state(ctx, st);
+    OFB_CHECK(cudaEventRecord(e1, s));
+    // loss 1/2 |u(T) - target|^2 on the unique entries and its seed
+    for(int c = 0; c < 3; ++c) {
+      zero(ctx, W->lam_vel[c], 1 + c);
+      zero(ctx, W->lam_prev[c], 1 + c);
+    }
+    zero(ctx, W->lam_p, 0);
+    const double* vel_t[3] = {st.vel[0], st.vel[1], st.vel[2]};
+    const double* tgt[3] = {W->target[0], W->target[1], W->target[2]};
+    ofb::launch_loss_seed(g, ctx->bc, vel_t, tgt, W->lam_vel, W->acc, ctx->rb, s);
+    // backward over the segments: recompute the states of a segment from its
+    // checkpoint, then run the reverse steps
+    const int nseg = (steps + every - 1) / every;
+    StepState ws{};
+    for(int c = 0; c < 3; ++c) {
+      ws.vel[c] = W->w_vel[c];
+      ws.adv_prev[c] = W->w_adv_prev[c];
+      ws.adv_cur[c] = W->w_adv_cur[c];
+      ws.corrected[c] = W->w_corr[c];
+    }
+    ws.p = W->w_p;
+    for(int k = nseg - 1; k >= 0; --k) {
+      const int n0 = k * every;
+      const int n1 = std::min(steps, n0 + every);
+      load_state(ctx, W->ckpt[k], ws);
+      for(int n = n0; n < n1; ++n) {
+        save_state(ctx, ws, W->seg[n - n0]);
+        if(n + 1 < n1) {
+          forward_step(ctx, prm, name, n + 1, ws);
+          ++forward_steps;
+        }
+      }
+      for(int n = n1 - 1; n >= n0; --n) adjoint_step(ctx, prm, W, W->seg[n - n0]);
+    }
+    // the initial state's ghosts were filled from its active entries
+    if(W->ckpt[0].clean) ofb::launch_velocity_bc_T(g, W->lam_vel[0], W->lam_vel[1], W->lam_vel[2], s);
+    for(int c = 0; c < 3; ++c) {
+      zero(ctx, W->out[c], 1 + c);
+      ofb::launch_axpby_active(g, ofb::kFaceX + c, 1.0, W->lam_vel[c], 0.0, nullptr, W->out[c], s);
+      ctx->download(gout[c], W->out[c], 1 + c);
+    }
+    OFB_CHECK(cudaEventRecord(e2, s));
+    double acc[4];
+    OFB_CHECK(cudaMemcpyAsync(acc, W->acc, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    ctx->sync();
+    if(info != nullptr) {
+      info->loss = acc[0];
+      info->grad_viscosity = acc[1] + 0.5 * prm->dt * acc[2];
+      info->forward_steps = forward_steps;
+      float f_ms = 0.0f, b_ms = 0.0f;
+      OFB_CHECK(cudaEventElapsedTime(&f_ms, e0, e1));
+      OFB_CHECK(cudaEventElapsedTime(&b_ms, e1, e2));
+      info->forward_ms = f_ms;
+      info->backward_ms = b_ms;
+      info->device_bytes = W->bytes;
+    }
   });
 }
 

@@ -71,6 +71,9 @@ struct PredictorArgs {
   int variant;            // 0 Taylor-Green, 1 cavity
 };
 void launch_predictor_rhs(const PredictorArgs& a, cudaStream_t s);
+// The predictor rhs from a.adv already computed (everything but the advection);
+// linear in (cur, p, adv, prev).
+void launch_predictor_rest(const PredictorArgs& a, cudaStream_t s);
 void launch_advection(const Grid& g, const double* u, const double* v, const double* w,
                       double* au, double* av, double* aw, cudaStream_t s);
 void launch_tg_init(const Grid& g, int mode, double* u, double* v, double* w, double* p,
@@ -141,6 +144,51 @@ void poisson_solve(PoissonPlan* p, int max_iterations, double tolerance, SolveSc
 // Writes x - sx into the active entries of a padded pressure field.
 void launch_compact_to_pressure(const Grid& g, const double* x, const SolveScalars* sc,
                                 double* p_padded, cudaStream_t s);
+
+// ---- tangent-linear and adjoint pieces (adjoint.cu), periodic grids ----
+// out = A'(base) dir: the advection's Jacobian-vector product (branches frozen).
+void launch_advection_jvp(const Grid& g, const double* const* base, const double* const* dir,
+                          double* const* out, cudaStream_t s);
+// lam_cur += A'(base)^T lam_adv (atomics; ghost positions included).
+void launch_advection_vjp(const Grid& g, const double* const* base, const double* const* lam_adv,
+                          double* const* lam_cur, cudaStream_t s);
+// lam_cur += W^T lam_rhs (the predictor's 27-point operator on the velocity)
+// and lam_p += (-dt G)^T lam_rhs (cells, ghosts included).
+void launch_predictor_T(const Grid& g, double nu, double dt, double alpha, const double* const* lam_rhs,
+                        double* const* lam_cur, double* lam_p, cudaStream_t s);
+// *acc += lam_rhs . d(rhs)/d(nu) at the base velocity cur.
+void launch_predictor_nu_dot(const Grid& g, double dt, double alpha, const double* const* cur,
+                             const double* const* lam_rhs, double* acc, RedBuf rb, cudaStream_t s);
+// out = a x + b y on the active entries of a padded field at `loc` (y may be null).
+void launch_axpby_active(const Grid& g, int loc, double a, const double* x, double b,
+                         const double* y, double* out, cudaStream_t s);
+// Transposes of the periodic velocity and total-pressure ghost fills.
+void launch_velocity_bc_T(const Grid& g, double* u, double* v, double* w, cudaStream_t s);
+void launch_component_bc_T(const Grid& g, int comp, double* f, cudaStream_t s);
+void launch_pressure_bc_T(const Grid& g, double* p, cudaStream_t s);
+// Duplicated periodic face of the normal component: fold into the first
+// unknown (fold) and clear, or just clear.
+void launch_duplicate(const Grid& g, int comp, bool fold, double* f, cudaStream_t s);
+// *acc += sum over lines of mu . D y (cyclic second difference on the unknowns).
+void launch_adi_alpha_dot(const Grid& g, int comp, int axis, int begin, int n, const double* mu,
+                          const double* y, double* acc, RedBuf rb, cudaStream_t s);
+// lam_pred += (scale D)^T lam_q ; lam_phi += (scale G_periodic)^T lam_corr.
+void launch_divergence_T(const Grid& g, double scale, const double* lam_q, double* const* lam_pred,
+                         cudaStream_t s);
+void launch_correct_T(const Grid& g, double scale, const double* const* lam_corr, double* lam_phi,
+                      cudaStream_t s);
+// lam = vel - target on the unique active entries; *loss += 1/2 |lam|^2.
+void launch_loss_seed(const Grid& g, const VBC& bc, const double* const* vel,
+                      const double* const* target, double* const* lam, double* loss, RedBuf rb,
+                      cudaStream_t s);
+// lam_q += x - sc->sx on the active cells.
+void launch_add_compact(const Grid& g, const double* x, const SolveScalars* sc, double* lam_q,
+                        cudaStream_t s);
+// *acc += scale * sum over active entries of a * b.
+void launch_dot_active(const Grid& g, int loc, const double* a, const double* b, double scale,
+                       double* acc, RedBuf rb, cudaStream_t s);
+// Geometry of one ADI sweep (begin, unknowns) for the viscosity derivative.
+void adi_axis_geometry(const AdiPlan* p, int comp, int axis, int* begin, int* n);
 
 // ---- allocation-free pressure rhs (noalloc.cu) ----
 // Device address of the file-scope scratch on the current device (looked up

@@ -222,13 +222,19 @@ void launch_predictor_rhs(const PredictorArgs& a, cudaStream_t s) {
     k_advect_bf<2><<<l2.grid, l2.block, 0, s>>>(a.g, a.cur[0], a.cur[1], a.cur[2], a.adv[2], l2.kchunk);
     OFB_LAUNCH_CHECK("k_advect_bf");
   }
-  {
-    ProfScope ps(kKPredictor, s, 3);
-    k_predictor_rest<0><<<l0.grid, l0.block, 0, s>>>(a, l0.kchunk);
-    k_predictor_rest<1><<<l1.grid, l1.block, 0, s>>>(a, l1.kchunk);
-    k_predictor_rest<2><<<l2.grid, l2.block, 0, s>>>(a, l2.kchunk);
-    OFB_LAUNCH_CHECK("k_predictor_rest");
-  }
+  launch_predictor_rest(a, s);
+}
+
+void launch_predictor_rest(const PredictorArgs& a, cudaStream_t s) {
+  const Lay Lu = make_lay(a.g, kFaceX), Lv = make_lay(a.g, kFaceY), Lw = make_lay(a.g, kFaceZ);
+  const Launch3 l0 = launch3(Lu.nx, Lu.ny, Lu.nz);
+  const Launch3 l1 = launch3(Lv.nx, Lv.ny, Lv.nz);
+  const Launch3 l2 = launch3(Lw.nx, Lw.ny, Lw.nz);
+  ProfScope ps(kKPredictor, s, 3);
+  k_predictor_rest<0><<<l0.grid, l0.block, 0, s>>>(a, l0.kchunk);
+  k_predictor_rest<1><<<l1.grid, l1.block, 0, s>>>(a, l1.kchunk);
+  k_predictor_rest<2><<<l2.grid, l2.block, 0, s>>>(a, l2.kchunk);
+  OFB_LAUNCH_CHECK("k_predictor_rest");
 }
 
 void launch_advection(const Grid& g, const double* u, const double* v, const double* w,

@@ -24,6 +24,7 @@ enum KernelClass : int {
   kKCorrect,
   kKCellPass,
   kKTotalPressureBc,
+  kKAdjoint,
   kKOther,
   kKernelCount
 };
