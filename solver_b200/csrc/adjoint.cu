@@ -503,14 +503,14 @@ __global__ void __launch_bounds__(kTX* kTY)
 
 // lam_q += x - sx on the active cells (the adjoint pressure solve's result).
 __global__ void k_add_compact(Grid g, const double* __restrict__ x, const SolveScalars* sc,
-                              double* lam_q) {
+                              double scale, double* lam_q) {
   const Lay P = make_lay(g, kCell);
   const CLay C = make_clay(g.nx, g.ny, g.nz);
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int k = blockIdx.z;
   if(i >= g.nx || j >= g.ny) return;
-  lam_q[P.idx(i + 1, j + 1, k + 1)] += x[C.idx(i, j, k)] - sc->sx;
+  lam_q[P.idx(i + 1, j + 1, k + 1)] += scale * (x[C.idx(i, j, k)] - sc->sx);
 }
 
 // sum over active cells of a * b (reduction into *acc).
@@ -741,12 +741,12 @@ void launch_loss_seed(const Grid& g, const VBC& bc, const double* const* vel,
   OFB_LAUNCH_CHECK("k_loss_seed");
 }
 
-void launch_add_compact(const Grid& g, const double* x, const SolveScalars* sc, double* lam_q,
-                        cudaStream_t s) {
+void launch_add_compact(const Grid& g, const double* x, const SolveScalars* sc, double scale,
+                        double* lam_q, cudaStream_t s) {
   dim3 block(32, 8, 1);
   dim3 grid((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz);
   ProfScope ps(kKAdjoint, s);
-  k_add_compact<<<grid, block, 0, s>>>(g, x, sc, lam_q);
+  k_add_compact<<<grid, block, 0, s>>>(g, x, sc, scale, lam_q);
   OFB_LAUNCH_CHECK("k_add_compact");
 }
 

@@ -181,9 +181,9 @@ void launch_correct_T(const Grid& g, double scale, const double* const* lam_corr
 void launch_loss_seed(const Grid& g, const VBC& bc, const double* const* vel,
                       const double* const* target, double* const* lam, double* loss, RedBuf rb,
                       cudaStream_t s);
-// lam_q += x - sc->sx on the active cells.
-void launch_add_compact(const Grid& g, const double* x, const SolveScalars* sc, double* lam_q,
-                        cudaStream_t s);
+// lam_q += scale (x - sc->sx) on the active cells.
+void launch_add_compact(const Grid& g, const double* x, const SolveScalars* sc, double scale,
+                        double* lam_q, cudaStream_t s);
 // *acc += scale * sum over active entries of a * b.
 void launch_dot_active(const Grid& g, int loc, const double* a, const double* b, double scale,
                        double* acc, RedBuf rb, cudaStream_t s);
