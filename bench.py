@@ -17,6 +17,13 @@ Arms:
                           in place; the plain-C oracle port if that build is
                           absent), one process per host core.
 
+The FP64 1-GPU line also carries two measurements of the rest of the
+headline metric (skip with --no-extras): "mixed" -- the mixed path's steps/s
+on the same workload, its speed-up, and its max-norm relative velocity
+difference from the FP64 path after 200 steps; "adjoint" -- the adjoint check
+workload (128^3, nu = 0.01, perturbed Taylor-Green, 100 steps, checkpoint
+every 10): adjoint/forward device-time ratio and a central-difference check.
+
 Multi-GPU: the path does not shard (replicas only): each rank runs its own
 independent 256^3 simulation; value = total steps/s over ranks, time = max
 over ranks.
@@ -405,6 +412,10 @@ def run_b200_arm(args, world, rank, local):
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(n, args.cpu_sample_n)
+    if world == 1 and args.precision == "fp64" and not args.no_extras:
+        ctx.close()
+        line["mixed"] = mixed_extra(n, dt, args, value)
+        line["adjoint"] = adjoint_extra()
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()
@@ -412,6 +423,107 @@ def run_b200_arm(args, world, rank, local):
         barrier()
         dist.destroy_process_group()
     return 0
+
+
+def timed_steps(ctx, prm, steps, stream):
+    """Device time (ms) of `steps` resident steps, CUDA events on the context stream."""
+    import torch
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    ctx.run_steps(prm, steps)
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def mixed_extra(n, dt, args, fp64_value, error_steps=200):
+    """The mixed path on the same workload: steps/s (same timing as the main
+    line), the speed-up over the FP64 value, and the max-norm relative
+    velocity difference from the FP64 path after `error_steps` steps from the
+    same initial state."""
+    import numpy as np
+    import torch
+    import solver_b200 as sb
+    h = 2.0 * math.pi / n
+    grid = sb.Grid(n, n, n, h, h, h)
+    prm = sb.step_params(NU, dt, MAX_IT, TOL)
+    out = {}
+    with sb.Context(grid, [sb.PERIODIC] * 6, precision=sb.OF_MIXED) as ctx:
+        stream = torch.cuda.ExternalStream(sb.context_stream(ctx))
+        ctx.tg_init(NU, dt, mode=1)
+        for _ in range(args.warmup):
+            ctx.run_steps(prm, 1)
+        ms = timed_steps(ctx, prm, args.steps, stream)
+        out["value"] = args.steps / (ms / 1000.0)
+        out["unit"] = "steps/s"
+        out["speedup_vs_fp64"] = out["value"] / fp64_value
+        ctx.tg_init(NU, dt, mode=1)
+        ctx.run_steps(prm, error_steps)
+        mixed = ctx.download_state()
+    with sb.Context(grid, [sb.PERIODIC] * 6) as ctx:
+        ctx.tg_init(NU, dt, mode=1)
+        ctx.run_steps(prm, error_steps)
+        ref = ctx.download_state()
+    err = max(float(np.max(np.abs(mixed[c][1:-1, 1:-1, 1:-1] - ref[c][1:-1, 1:-1, 1:-1])))
+              for c in "uvw") / max(float(np.max(np.abs(ref[c][1:-1, 1:-1, 1:-1]))) for c in "uvw")
+    out["rel_velocity_error_vs_fp64"] = err
+    out["error_steps"] = error_steps
+    out["precision"] = "FP32 V-cycle (storage and arithmetic) inside the FP64 CG"
+    return out
+
+
+def adjoint_extra(n=128, steps=100, every=10, viscosity=0.01):
+    """The adjoint check workload: Taylor-Green plus a seeded solenoidal
+    perturbation (Fourier modes |k| <= 4, RMS 1e-2, projected), loss
+    1/2 |u(T) - u_target|^2 with the target from another seed's forward run,
+    `steps` steps, checkpoint every `every`.  Reports the adjoint/forward
+    device-time ratio and a central-difference check of the gradient along a
+    smooth direction (eps = 1e-8)."""
+    import numpy as np
+    import torch
+    import solver_b200 as sb
+    from solver_b200.adjoint import perturbed_taylor_green, smooth_field, unique_loss, upload_initial
+    h = 2.0 * math.pi / n
+    grid = sb.Grid(n, n, n, h, h, h)
+    dt = tg_dt(n)
+    prm = sb.step_params(viscosity, dt, MAX_IT, TOL)
+    with sb.Context(grid, [sb.PERIODIC] * 6) as ctx:
+        stream = torch.cuda.ExternalStream(sb.context_stream(ctx))
+        state = perturbed_taylor_green(ctx, viscosity, dt, seed=1)
+        other = perturbed_taylor_green(ctx, viscosity, dt, seed=2)
+        upload_initial(ctx, other)
+        ctx.run_steps(prm, steps)
+        tst = ctx.download_state()
+        target = [tst[c] for c in "uvw"]
+        upload_initial(ctx, state)
+        ctx.run_steps(prm, 2)
+        upload_initial(ctx, state)
+        fwd_ms = timed_steps(ctx, prm, steps, stream)
+        upload_initial(ctx, state)
+        grad, info = ctx.adjoint_gradient(prm, steps, target, checkpoint_every=every)
+        d = smooth_field(grid, 5)
+        eps = 1e-8
+        loss = []
+        for sgn in (1.0, -1.0):
+            upload_initial(ctx, (state[0] + sgn * eps * d[0], state[1] + sgn * eps * d[1],
+                                 state[2] + sgn * eps * d[2], state[3]))
+            ctx.run_steps(prm, steps)
+            st = ctx.download_state()
+            loss.append(unique_loss([st[c] for c in "uvw"], target))
+        fd = (loss[0] - loss[1]) / (2 * eps)
+        ad = sum(float(np.sum(d[i][1:-1, 1:-1, 1:-1] * grad[i][1:-1, 1:-1, 1:-1])) for i in range(3))
+    return {"workload": f"taylor_green_3d_{n}_perturbed", "steps": steps, "checkpoint_every": every,
+            "viscosity": viscosity, "forward_ms": fwd_ms,
+            "adjoint_ms": info["forward_ms"] + info["backward_ms"],
+            "ratio_adjoint_over_forward": (info["forward_ms"] + info["backward_ms"]) / fwd_ms,
+            "forward_steps_run": info["forward_steps"], "loss": info["loss"],
+            "grad_viscosity": info["grad_viscosity"],
+            "fd_check": {"direction": "smooth, |k| <= 4", "eps": eps, "fd": fd, "adjoint": ad,
+                         "rel_error": abs(fd - ad) / abs(fd)},
+            "device_bytes": info["device_bytes"],
+            "timing": "CUDA events; adjoint = first forward pass + segment recomputation + reverse steps"}
 
 
 def main():
@@ -426,6 +538,8 @@ def main():
     ap.add_argument("--profile-steps", type=int, default=2)
     ap.add_argument("--cpu-sample-n", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the mixed-precision and adjoint measurements of the FP64 1-GPU line")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")
