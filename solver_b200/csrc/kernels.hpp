@@ -36,6 +36,7 @@ struct SolveScalars {
   int body_runs;
   double* hist;   // device residual history, hist[0] = r0
   int hist_cap;
+  int outer;      // mixed path: defect-correction steps taken
 };
 
 // Per-level mean shifts of the V-cycle vectors.

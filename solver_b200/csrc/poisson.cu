@@ -503,11 +503,12 @@ __global__ void __launch_bounds__(256)
   reduce_finish<1>(acc, mx, rb, [=](const Sums<1>& s) { ls->sa = zm ? s.v[0] / n : 0.0; });
 }
 
-// A p; same contract as k_apply_ap.
+// A p; same contract as k_apply_ap.  V is the vector type (arithmetic FP64).
+template <typename V>
 __global__ void __launch_bounds__(256)
-    k_vapply_ap(OpInfo o, const double* __restrict__ p, double* __restrict__ ap, SolveScalars* sc,
+    k_vapply_ap(OpInfo o, const V* __restrict__ p, V* __restrict__ ap, SolveScalars* sc,
                 int kchunk, RedBuf rb) {
-  ROW_PROLOGUE(double)
+  ROW_PROLOGUE(V)
   using R = vst::Row<double, W>;
   const double sp = sc->sp;
   double acc[3] = {0.0, 0.0, 0.0};
@@ -519,11 +520,11 @@ __global__ void __launch_bounds__(256)
         for(int t = 0; t < W; ++t) r.v[t] -= sp;
         return r;
       },
-      [&](int ii, int jj, int kk) { return p[o.L.idx(ii, jj, kk)] - sp; },
+      [&](int ii, int jj, int kk) { return double(p[o.L.idx(ii, jj, kk)]) - sp; },
       [&](int, int, int) { return 0; },
       [&](int k, const R& c, const R& ax, int) {
         if(g.act) {
-          vst::st<double, W>(ap + o.L.idx(g.i0, g.j, k), ax);
+          vst::st<V, W>(ap + o.L.idx(g.i0, g.j, k), ax);
 #pragma unroll
           for(int t = 0; t < W; ++t) {
             acc[0] += ax.v[t];
@@ -939,9 +940,10 @@ __global__ void __launch_bounds__(kTailThreads)
 // ---------------------------------------------------------------------------
 
 // r = (b - sb) - A (x - sx); initial residual (linsolve/poisson_solver.cpp:717-739).
+template <typename V>
 __global__ void __launch_bounds__(kTX* kTY)
-    k_initial_residual(OpInfo o, const double* __restrict__ b, const double* __restrict__ x,
-                       double* __restrict__ r, SolveScalars* sc, int kchunk, RedBuf rb,
+    k_initial_residual(OpInfo o, const V* __restrict__ b, const V* __restrict__ x,
+                       V* __restrict__ r, SolveScalars* sc, int kchunk, RedBuf rb,
                        cudaGraphConditionalHandle cond) {
   STENCIL_PROLOGUE(o.L)
   const double sb = sc->sb, sx = sc->sx;
@@ -949,16 +951,16 @@ __global__ void __launch_bounds__(kTX* kTY)
   zero(acc);
   if(valid) {
     const ColNb nb = col_nb(o, i, j);
-    auto val = [&](int ii, int jj, int kk) { return x[o.L.idx(ii, jj, kk)] - sx; };
+    auto val = [&](int ii, int jj, int kk) { return double(x[o.L.idx(ii, jj, kk)]) - sx; };
     k_batched<kBatch>(
         k0, k1,
         [&](int k) {
           double c;
           const double ax = apply_op<double>(o, nb, i, j, k, val, c);
-          return (b[o.L.idx(i, j, k)] - sb) - ax;
+          return (double(b[o.L.idx(i, j, k)]) - sb) - ax;
         },
         [&](int k, double v) {
-          r[o.L.idx(i, j, k)] = v;
+          r[o.L.idx(i, j, k)] = V(v);
           acc[0] += v;
           acc[1] += v * v;
         });
@@ -987,9 +989,9 @@ __global__ void __launch_bounds__(kTX* kTY)
 }
 
 // p = (z - sz) + beta (p - sp); first iteration p = z - sz.
-template <typename T>
+template <typename T, typename V>
 __global__ void __launch_bounds__(kTX* kTY)
-    k_update_p(CLay L, const T* __restrict__ z, const LevelScalars* ls0, double* __restrict__ p,
+    k_update_p(CLay L, const T* __restrict__ z, const LevelScalars* ls0, V* __restrict__ p,
                SolveScalars* sc, int kchunk, RedBuf rb) {
   STENCIL_PROLOGUE(L)
   const int first = sc->first;
@@ -1003,10 +1005,10 @@ __global__ void __launch_bounds__(kTX* kTY)
         k0, k1,
         [&](int k) {
           const int q = L.idx(i, j, k);
-          return first ? double(z[q]) - sz : (double(z[q]) - sz) + beta * (p[q] - sp);
+          return first ? double(z[q]) - sz : (double(z[q]) - sz) + beta * (double(p[q]) - sp);
         },
         [&](int k, double v) {
-          p[L.idx(i, j, k)] = v;
+          p[L.idx(i, j, k)] = V(v);
           acc[0] += v;
         });
   }
@@ -1018,8 +1020,9 @@ __global__ void __launch_bounds__(kTX* kTY)
 }
 
 // Ap = A (p - sp); mean shift of Ap; p.Ap; alpha (linsolve/poisson_solver.cpp:751-761).
+template <typename V>
 __global__ void __launch_bounds__(kTX* kTY)
-    k_apply_ap(OpInfo o, const double* __restrict__ p, double* __restrict__ ap, SolveScalars* sc,
+    k_apply_ap(OpInfo o, const V* __restrict__ p, V* __restrict__ ap, SolveScalars* sc,
                int kchunk, RedBuf rb) {
   STENCIL_PROLOGUE(o.L)
   const double sp = sc->sp;
@@ -1027,7 +1030,7 @@ __global__ void __launch_bounds__(kTX* kTY)
   zero(acc);
   if(valid) {
     const ColNb nb = col_nb(o, i, j);
-    auto val = [&](int ii, int jj, int kk) { return p[o.L.idx(ii, jj, kk)] - sp; };
+    auto val = [&](int ii, int jj, int kk) { return double(p[o.L.idx(ii, jj, kk)]) - sp; };
     k_batched<kBatch>(
         k0, k1,
         [&](int k) {
@@ -1036,7 +1039,7 @@ __global__ void __launch_bounds__(kTX* kTY)
           return Pair<double>{v, c};
         },
         [&](int k, Pair<double> r) {
-          ap[o.L.idx(i, j, k)] = r.v;
+          ap[o.L.idx(i, j, k)] = V(r.v);
           acc[0] += r.v;
           acc[1] += r.w * r.v;
           acc[2] += r.w;
@@ -1058,9 +1061,10 @@ __global__ void __launch_bounds__(kTX* kTY)
 
 // x = (x - sx) + alpha (p - sp); r = (r - sr) - alpha (Ap - sap); norms and
 // the convergence test (linsolve/poisson_solver.cpp:762-782).
+template <typename V>
 __global__ void __launch_bounds__(kTX* kTY)
-    k_update_xr(CLay L, double* __restrict__ x, double* __restrict__ r,
-                const double* __restrict__ p, const double* __restrict__ ap, SolveScalars* sc,
+    k_update_xr(CLay L, V* __restrict__ x, V* __restrict__ r,
+                const V* __restrict__ p, const V* __restrict__ ap, SolveScalars* sc,
                 int kchunk, RedBuf rb, cudaGraphConditionalHandle cond) {
   STENCIL_PROLOGUE(L)
   const int stop = sc->stop;
@@ -1072,12 +1076,13 @@ __global__ void __launch_bounds__(kTX* kTY)
         k0, k1,
         [&](int k) {
           const int q = L.idx(i, j, k);
-          return Pair<double>{(x[q] - sx) + alpha * (p[q] - sp), (r[q] - sr) - alpha * (ap[q] - sap)};
+          return Pair<double>{(double(x[q]) - sx) + alpha * (double(p[q]) - sp),
+                              (double(r[q]) - sr) - alpha * (double(ap[q]) - sap)};
         },
         [&](int k, Pair<double> v) {
           const int q = L.idx(i, j, k);
-          x[q] = v.v;
-          r[q] = v.w;
+          x[q] = V(v.v);
+          r[q] = V(v.w);
           acc[0] += v.v;
           acc[1] += v.w;
           acc[2] += v.w * v.w;
@@ -1106,6 +1111,122 @@ __global__ void __launch_bounds__(kTX* kTY)
     // the reference's loop: at most max_iterations iterations, stop on convergence
     sc->cont = (sc->converged || sc->iterations >= sc->max_it) ? 0 : 1;
     if(cond) cudaGraphSetConditional(cond, sc->cont);
+  });
+}
+
+// Mixed path: the FP64 residual scaled to unit RMS into the FP32 inner rhs,
+// the inner correction cleared, and the inner loop's scalars initialised the
+// way k_initial_residual does it for a zero initial guess.
+__global__ void __launch_bounds__(kTX* kTY)
+    k_dc_to_inner(CLay L, const double* __restrict__ r, const SolveScalars* sc,
+                  float* __restrict__ r32, float* __restrict__ e32, SolveScalars* si, int kchunk,
+                  RedBuf rb, cudaGraphConditionalHandle cond) {
+  STENCIL_PROLOGUE(L)
+  const double sr = sc->sr;
+  const double inv = sc->rnorm > 0.0 ? 1.0 / sc->rnorm : 1.0;
+  double acc[2];
+  zero(acc);
+  if(valid) {
+    for(int k = k0; k < k1; ++k) {
+      const int q = L.idx(i, j, k);
+      const float v = float((r[q] - sr) * inv);
+      r32[q] = v;
+      e32[q] = 0.0f;
+      acc[0] += double(v);
+      acc[1] += double(v) * double(v);
+    }
+  }
+  const bool mx[2] = {false, false};
+  reduce_finish<2>(acc, mx, rb, [=](const Sums<2>& s) {
+    const int n = si->n;
+    const double srn = si->zero_mean ? s.v[0] / n : 0.0;
+    si->sr = srn;
+    si->sum_r = s.v[0];
+    const double r0 = sqrt(fmax(s.v[1] - n * srn * srn, 0.0) / n);
+    si->r0 = r0;
+    si->rnorm = r0;
+    si->rel = 1.0;
+    si->iterations = 0;
+    si->stop = 0;
+    si->converged = 0;
+    si->first = 1;
+    si->body_runs = 0;
+    si->sx = 0.0;
+    si->sp = 0.0;
+    si->hist = nullptr;
+    si->hist_cap = 0;
+    si->cont = r0 > 0.0 ? 1 : 0;
+    if(cond) cudaGraphSetConditional(cond, si->cont);
+  });
+}
+
+// Mixed path: x = (x - sx) + scale (e - sx_inner) with the scale the inner
+// rhs was divided by; records mean(x).
+__global__ void __launch_bounds__(kTX* kTY)
+    k_dc_update_x(CLay L, double* __restrict__ x, const float* __restrict__ e32, SolveScalars* sc,
+                  const SolveScalars* si, int kchunk, RedBuf rb) {
+  STENCIL_PROLOGUE(L)
+  const double scale = sc->rnorm > 0.0 ? sc->rnorm : 1.0;
+  const double sx = sc->sx, sxi = si->sx;
+  double acc[1];
+  zero(acc);
+  if(valid) {
+    for(int k = k0; k < k1; ++k) {
+      const int q = L.idx(i, j, k);
+      const double v = (x[q] - sx) + scale * (double(e32[q]) - sxi);
+      x[q] = v;
+      acc[0] += v;
+    }
+  }
+  const bool mx[1] = {false};
+  reduce_finish<1>(acc, mx, rb, [=](const Sums<1>& s) {
+    sc->sx = sc->zero_mean ? s.v[0] / sc->n : 0.0;
+  });
+}
+
+// Mixed path: the FP64 residual r = (b - sb) - A (x - sx) after a correction,
+// its norm, the convergence test against the reference's relative tolerance
+// and the loop control (the total of inner iterations is the iteration count).
+__global__ void __launch_bounds__(kTX* kTY)
+    k_dc_residual(OpInfo o, const double* __restrict__ b, const double* __restrict__ x,
+                  double* __restrict__ r, SolveScalars* sc, const SolveScalars* si, int kchunk,
+                  RedBuf rb) {
+  STENCIL_PROLOGUE(o.L)
+  const double sb = sc->sb, sx = sc->sx;
+  double acc[2];
+  zero(acc);
+  if(valid) {
+    const ColNb nb = col_nb(o, i, j);
+    auto val = [&](int ii, int jj, int kk) { return x[o.L.idx(ii, jj, kk)] - sx; };
+    k_batched<kBatch>(
+        k0, k1,
+        [&](int k) {
+          double c;
+          const double ax = apply_op<double>(o, nb, i, j, k, val, c);
+          return (b[o.L.idx(i, j, k)] - sb) - ax;
+        },
+        [&](int k, double v) {
+          r[o.L.idx(i, j, k)] = v;
+          acc[0] += v;
+          acc[1] += v * v;
+        });
+  }
+  const bool mx[2] = {false, false};
+  reduce_finish<2>(acc, mx, rb, [=](const Sums<2>& s) {
+    const int n = sc->n;
+    const double srn = sc->zero_mean ? s.v[0] / n : 0.0;
+    sc->sr = srn;
+    sc->sum_r = s.v[0];
+    const double rn = sqrt(fmax(s.v[1] - n * srn * srn, 0.0) / n);
+    sc->rnorm = rn;
+    sc->iterations += si->iterations;
+    sc->body_runs += si->body_runs;
+    sc->outer += 1;
+    sc->rel = sc->r0 > 0.0 ? rn / sc->r0 : 0.0;
+    if(sc->rel <= sc->tol) sc->converged = 1;
+    if(sc->hist != nullptr && sc->outer < sc->hist_cap) sc->hist[sc->outer] = rn;
+    const bool stalled = si->iterations == 0;
+    sc->cont = (sc->converged || sc->iterations >= sc->max_it || sc->outer >= 100 || stalled) ? 0 : 1;
   });
 }
 
@@ -1157,6 +1278,9 @@ struct PoissonPlan {
   cudaGraphExec_t exec = nullptr;
   long long pre_counts[kKernelCount] = {};
   long long body_counts[kKernelCount] = {};
+  // mixed path: inner (FP32) CG vectors and scalars
+  float *r32 = nullptr, *e32 = nullptr, *p32 = nullptr, *ap32 = nullptr;
+  SolveScalars* sc_in = nullptr;
   // levels tail_first.. run as one single-block launch (k_vcycle_tail)
   int tail_first = -1;
   TailArgs tail{};
@@ -1424,6 +1548,15 @@ PoissonPlan* poisson_plan_create(const Grid& g, const PBC& pbc_in, int precision
   OFB_CHECK(cudaMalloc(&P->ap, nf * sizeof(double)));
   OFB_CHECK(cudaMemset(P->p, 0, nf * sizeof(double)));
   P->bytes += 5 * nf * sizeof(double);
+  if(precision == 1) {
+    for(float** v : {&P->r32, &P->e32, &P->p32, &P->ap32}) {
+      OFB_CHECK(cudaMalloc(v, nf * sizeof(float)));
+      OFB_CHECK(cudaMemset(*v, 0, nf * sizeof(float)));
+    }
+    OFB_CHECK(cudaMalloc(&P->sc_in, sizeof(SolveScalars)));
+    OFB_CHECK(cudaMemset(P->sc_in, 0, sizeof(SolveScalars)));
+    P->bytes += 4 * nf * sizeof(float);
+  }
   const char* no_graph = std::getenv("ORCHARD_B200_NO_GRAPH");
   P->use_graph = !(no_graph != nullptr && no_graph[0] == '1');
   return P;
@@ -1448,6 +1581,11 @@ void poisson_plan_destroy(PoissonPlan* P) {
   cudaFree(P->r);
   cudaFree(P->p);
   cudaFree(P->ap);
+  cudaFree(P->r32);
+  cudaFree(P->e32);
+  cudaFree(P->p32);
+  cudaFree(P->ap32);
+  cudaFree(P->sc_in);
   delete P;
 }
 
@@ -1486,9 +1624,9 @@ void launch_restrict(const Level& lv, const Level& cv, const B* b, const double*
 }
 
 // v_cycle (linsolve/poisson_solver.cpp:597-633) from level l; the finest
-// level's rhs is the CG residual (double, shift sc->sr).
-template <typename T>
-void v_cycle(PoissonPlan* P, int l, SolveScalars* sc, RedBuf rb, cudaStream_t s) {
+// level's rhs is the CG residual r0 (type V, shift sc->sr).
+template <typename T, typename V>
+void v_cycle(PoissonPlan* P, int l, const V* r0, SolveScalars* sc, RedBuf rb, cudaStream_t s) {
   Level& lv = P->levels[l];
   const int nl = static_cast<int>(P->levels.size());
   const int zm = P->zero_mean;
@@ -1507,8 +1645,8 @@ void v_cycle(PoissonPlan* P, int l, SolveScalars* sc, RedBuf rb, cudaStream_t s)
   if(l + 1 == nl) {
     ProfScope ps(kKCoarseSolve, s);
     if(l == 0)
-      k_coarse_solve<T, double><<<1, 256, 0, s>>>(P->coarse_n, P->swaps, P->factors, P->r, sb_ptr,
-                                                  x, ls, zm, rz_sc);
+      k_coarse_solve<T, V><<<1, 256, 0, s>>>(P->coarse_n, P->swaps, P->factors, r0, sb_ptr, x, ls,
+                                             zm, rz_sc);
     else
       k_coarse_solve<T, T><<<1, 256, 0, s>>>(P->coarse_n, P->swaps, P->factors,
                                             static_cast<const T*>(lv.b), sb_ptr, x, ls, zm, rz_sc);
@@ -1556,7 +1694,7 @@ void v_cycle(PoissonPlan* P, int l, SolveScalars* sc, RedBuf rb, cudaStream_t s)
                               lc, rb, s);
     }
     OFB_LAUNCH_CHECK("v_cycle descent");
-    v_cycle<T>(P, l + 1, sc, rb, s);
+    v_cycle<T, V>(P, l + 1, r0, sc, rb, s);
     {
       ProfScope ps(fine ? kKProlongFine : kKCoarseLevels, s);
       if(vpr)
@@ -1579,17 +1717,27 @@ void v_cycle(PoissonPlan* P, int l, SolveScalars* sc, RedBuf rb, cudaStream_t s)
     }
     OFB_LAUNCH_CHECK("v_cycle ascent");
   };
-  if(l == 0) smooth_chain(static_cast<const double*>(P->r));
+  if(l == 0) smooth_chain(r0);
   else smooth_chain(static_cast<const T*>(lv.b));
 }
 
+// The vectors of one CG loop: FP64 for the reference's solve, FP32 for the
+// inner solves of the mixed path's defect correction.
+template <typename V>
+struct CGVec {
+  V *b, *x, *r, *p, *ap;
+};
+
+CGVec<double> cg64(PoissonPlan* P) { return CGVec<double>{P->b, P->x, P->r, P->p, P->ap}; }
+
 // Initial residual and convergence test (linsolve/poisson_solver.cpp:717-739).
-void enqueue_pre(PoissonPlan* P, SolveScalars* sc, RedBuf rb, cudaStream_t s,
+template <typename V>
+void enqueue_pre(PoissonPlan* P, const CGVec<V>& v, SolveScalars* sc, RedBuf rb, cudaStream_t s,
                  cudaGraphConditionalHandle cond) {
   const Level& l0 = P->levels[0];
   const Launch3 ln = launch3(l0.L.nx, l0.L.ny, l0.L.nz);
   ProfScope ps(kKInitResidual, s);
-  k_initial_residual<<<ln.grid, ln.block, 0, s>>>(l0.op, P->b, P->x, P->r, sc, ln.kchunk, rb, cond);
+  k_initial_residual<V><<<ln.grid, ln.block, 0, s>>>(l0.op, v.b, v.x, v.r, sc, ln.kchunk, rb, cond);
   OFB_LAUNCH_CHECK("k_initial_residual");
 }
 
@@ -1598,38 +1746,40 @@ void enqueue_pre(PoissonPlan* P, SolveScalars* sc, RedBuf rb, cudaStream_t s,
 // preconditioner moved to the top; the body count is the reference's
 // iteration count, and the first body forms p = z as the reference does
 // before its loop (:741-749).
-template <typename T>
-void enqueue_body(PoissonPlan* P, SolveScalars* sc, RedBuf rb, cudaStream_t s,
+template <typename T, typename V>
+void enqueue_body(PoissonPlan* P, const CGVec<V>& v, SolveScalars* sc, RedBuf rb, cudaStream_t s,
                   cudaGraphConditionalHandle cond) {
   const Level& l0 = P->levels[0];
   const Launch3 ln = launch3(l0.L.nx, l0.L.ny, l0.L.nz);
-  v_cycle<T>(P, 0, sc, rb, s);
+  v_cycle<T, V>(P, 0, v.r, sc, rb, s);
   {
     ProfScope ps(kKUpdateP, s);
-    k_update_p<T><<<ln.grid, ln.block, 0, s>>>(l0.L, static_cast<const T*>(l0.x), P->ls, P->p, sc,
-                                               ln.kchunk, rb);
+    k_update_p<T, V><<<ln.grid, ln.block, 0, s>>>(l0.L, static_cast<const T*>(l0.x), P->ls, v.p,
+                                                  sc, ln.kchunk, rb);
   }
   {
     ProfScope ps(kKApplyAp, s);
-    if(vfits<double>(l0.L) && vec_enabled() && vec_enabled("ap")) {
-      const vst::RowLaunch lr = vst::row_launch(l0.L.nx, l0.L.ny, l0.L.nz, 2, 16);
-      k_vapply_ap<<<lr.grid, lr.block, 0, s>>>(l0.op, P->p, P->ap, sc, lr.kchunk, rb);
+    if(vfits<V>(l0.L) && vec_enabled() && vec_enabled("ap")) {
+      const vst::RowLaunch lr = vst::row_launch(l0.L.nx, l0.L.ny, l0.L.nz, vst::Width<V>::W, 16);
+      k_vapply_ap<V><<<lr.grid, lr.block, 0, s>>>(l0.op, v.p, v.ap, sc, lr.kchunk, rb);
     }
     else
-      k_apply_ap<<<ln.grid, ln.block, 0, s>>>(l0.op, P->p, P->ap, sc, ln.kchunk, rb);
+      k_apply_ap<V><<<ln.grid, ln.block, 0, s>>>(l0.op, v.p, v.ap, sc, ln.kchunk, rb);
   }
   {
     ProfScope ps(kKUpdateXr, s);
-    k_update_xr<<<ln.grid, ln.block, 0, s>>>(l0.L, P->x, P->r, P->p, P->ap, sc, ln.kchunk, rb, cond);
+    k_update_xr<V><<<ln.grid, ln.block, 0, s>>>(l0.L, v.x, v.r, v.p, v.ap, sc, ln.kchunk, rb, cond);
   }
   OFB_LAUNCH_CHECK("pcg body");
 }
 
-// The whole solve as one graph: pre -> WHILE(cont) { body }.  The loop is
-// bounded by max_iterations (the body clears the condition), so the graph
+// A loop as one graph: pre -> WHILE(cont) { body }.  pre and body are
+// enqueue callbacks taking the conditional handle; the loop is bounded by the
+// iteration limit the body enforces (it clears the condition), so the graph
 // always terminates.
-template <typename T>
-void build_graph(PoissonPlan* P, SolveScalars* sc, RedBuf rb, cudaStream_t s) {
+template <typename Pre, typename Body>
+cudaGraphExec_t build_loop_graph(PoissonPlan* P, cudaStream_t s, Pre pre, Body body,
+                                 cudaGraph_t* graph_out) {
   cudaGraph_t g = nullptr;
   OFB_CHECK(cudaGraphCreate(&g, 0));
   cudaGraphConditionalHandle cond = 0;
@@ -1637,7 +1787,7 @@ void build_graph(PoissonPlan* P, SolveScalars* sc, RedBuf rb, cudaStream_t s) {
   for(int i = 0; i < kKernelCount; ++i) P->pre_counts[i] = P->body_counts[i] = 0;
   prof_capture_begin(P->pre_counts);
   OFB_CHECK(cudaStreamBeginCaptureToGraph(s, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-  enqueue_pre(P, sc, rb, s, cond);
+  pre(cond);
   cudaStreamCaptureStatus status;
   const cudaGraphNode_t* deps = nullptr;
   size_t ndeps = 0;
@@ -1652,60 +1802,77 @@ void build_graph(PoissonPlan* P, SolveScalars* sc, RedBuf rb, cudaStream_t s) {
   cp.conditional.size = 1;
   cudaGraphNode_t wnode;
   OFB_CHECK(cudaGraphAddNode(&wnode, g, leaf.data(), leaf.size(), &cp));
-  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  cudaGraph_t bodyg = cp.conditional.phGraph_out[0];
   prof_capture_begin(P->body_counts);
-  OFB_CHECK(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0,
+  OFB_CHECK(cudaStreamBeginCaptureToGraph(s, bodyg, nullptr, nullptr, 0,
                                           cudaStreamCaptureModeThreadLocal));
-  enqueue_body<T>(P, sc, rb, s, cond);
-  OFB_CHECK(cudaStreamEndCapture(s, &body));
+  body(cond);
+  OFB_CHECK(cudaStreamEndCapture(s, &bodyg));
   prof_capture_end();
-  OFB_CHECK(cudaGraphInstantiate(&P->exec, g, 0));
-  P->graph = g;
+  cudaGraphExec_t exec = nullptr;
+  OFB_CHECK(cudaGraphInstantiate(&exec, g, 0));
+  *graph_out = g;
+  return exec;
 }
 
-template <typename T>
-void solve_impl(PoissonPlan* P, int max_iterations, double tolerance, SolveScalars* sc,
-                SolveScalars* host, RedBuf rb, cudaStream_t s, double* history, int history_cap) {
-  const Level& l0 = P->levels[0];
+void ensure_history(PoissonPlan* P, int max_iterations) {
   if(P->hist_cap < max_iterations + 1) {
     if(P->hist) cudaFree(P->hist);
     P->hist = nullptr;
     OFB_CHECK(cudaMalloc(&P->hist, sizeof(double) * (max_iterations + 1)));
     P->hist_cap = max_iterations + 1;
   }
-  // sc->sb and sc->sx were set by the kernels that filled b and x.
+}
+
+// Host-side initialisation of the solve scalars (b and x shifts were set by
+// the kernels that filled them).
+SolveScalars init_scalars(PoissonPlan* P, int max_iterations, double tolerance, SolveScalars* sc,
+                          SolveScalars* host, cudaStream_t s) {
   OFB_CHECK(cudaMemcpyAsync(host, sc, sizeof(SolveScalars), cudaMemcpyDeviceToHost, s));
   OFB_CHECK(cudaStreamSynchronize(s));
   SolveScalars init = *host;
   init.zero_mean = P->zero_mean;
-  init.n = l0.L.count();
+  init.n = P->levels[0].L.count();
   init.tol = tolerance;
   init.max_it = max_iterations;
   init.hist = P->hist;
   init.hist_cap = P->hist_cap;
+  init.outer = 0;
   if(!P->zero_mean) {
     init.sb = 0.0;
     init.sx = 0.0;
     init.removed_rhs_mean = 0.0;
   }
   init.sp = 0.0;
-  *host = init;
+  return init;
+}
+
+template <typename T>
+void solve_impl(PoissonPlan* P, int max_iterations, double tolerance, SolveScalars* sc,
+                SolveScalars* host, RedBuf rb, cudaStream_t s, double* history, int history_cap) {
+  ensure_history(P, max_iterations);
+  *host = init_scalars(P, max_iterations, tolerance, sc, host, s);
   OFB_CHECK(cudaMemcpyAsync(sc, host, sizeof(SolveScalars), cudaMemcpyHostToDevice, s));
+  const CGVec<double> v = cg64(P);
   const bool use_graph = P->use_graph && !prof_enabled();
   if(use_graph) {
-    if(P->exec == nullptr) build_graph<T>(P, sc, rb, s);
+    if(P->exec == nullptr)
+      P->exec = build_loop_graph(
+          P, s, [&](cudaGraphConditionalHandle c) { enqueue_pre<double>(P, v, sc, rb, s, c); },
+          [&](cudaGraphConditionalHandle c) { enqueue_body<T, double>(P, v, sc, rb, s, c); },
+          &P->graph);
     OFB_CHECK(cudaGraphLaunch(P->exec, s));
     OFB_CHECK(cudaMemcpyAsync(host, sc, sizeof(SolveScalars), cudaMemcpyDeviceToHost, s));
     OFB_CHECK(cudaStreamSynchronize(s));
     prof_add_counts(P->pre_counts, 1);
     prof_add_counts(P->body_counts, host->body_runs);
   } else {
-    enqueue_pre(P, sc, rb, s, 0);
+    enqueue_pre<double>(P, v, sc, rb, s, 0);
     OFB_CHECK(cudaMemcpyAsync(host, sc, sizeof(SolveScalars), cudaMemcpyDeviceToHost, s));
     OFB_CHECK(cudaStreamSynchronize(s));
     prof_collect();
     while(host->cont) {
-      enqueue_body<T>(P, sc, rb, s, 0);
+      enqueue_body<T, double>(P, v, sc, rb, s, 0);
       OFB_CHECK(cudaMemcpyAsync(host, sc, sizeof(SolveScalars), cudaMemcpyDeviceToHost, s));
       OFB_CHECK(cudaStreamSynchronize(s));
       prof_collect();
@@ -1717,13 +1884,99 @@ void solve_impl(PoissonPlan* P, int max_iterations, double tolerance, SolveScala
   }
 }
 
+// ---------------------------------------------------------------------------
+// Mixed path: defect correction.  The outer loop is FP64 -- residual
+// r = b - A x, its norm and the convergence test against the reference's
+// relative tolerance, the update x += e, the mean shifts -- and each inner
+// solve A e = r runs the same MG-PCG entirely in FP32 storage and arithmetic
+// (V-cycle and CG vectors; dot products and means accumulated in FP64) on the
+// residual scaled to unit RMS, to a relative residual of kInnerTol.  The
+// reported iteration count is the total number of inner iterations.
+// ---------------------------------------------------------------------------
+constexpr double kInnerTol = 1.0e-5;
+constexpr int kInnerMaxIt = 60;
+
+template <typename T>
+void solve_dc(PoissonPlan* P, int max_iterations, double tolerance, SolveScalars* sc,
+              SolveScalars* host, RedBuf rb, cudaStream_t s, double* history, int history_cap) {
+  ensure_history(P, max_iterations);
+  SolveScalars init = init_scalars(P, max_iterations, tolerance, sc, host, s);
+  *host = init;
+  OFB_CHECK(cudaMemcpyAsync(sc, host, sizeof(SolveScalars), cudaMemcpyHostToDevice, s));
+  SolveScalars in{};
+  in.zero_mean = P->zero_mean;
+  in.n = init.n;
+  in.tol = kInnerTol;
+  in.max_it = kInnerMaxIt;
+  OFB_CHECK(cudaMemcpyAsync(P->sc_in, &in, sizeof(SolveScalars), cudaMemcpyHostToDevice, s));
+  const Level& l0 = P->levels[0];
+  const Launch3 ln = launch3(l0.L.nx, l0.L.ny, l0.L.nz);
+  // outer residual of the initial guess
+  {
+    ProfScope ps(kKInitResidual, s);
+    k_initial_residual<double><<<ln.grid, ln.block, 0, s>>>(l0.op, P->b, P->x, P->r, sc, ln.kchunk,
+                                                            rb, 0);
+    OFB_LAUNCH_CHECK("k_initial_residual");
+  }
+  OFB_CHECK(cudaMemcpyAsync(host, sc, sizeof(SolveScalars), cudaMemcpyDeviceToHost, s));
+  OFB_CHECK(cudaStreamSynchronize(s));
+  const CGVec<float> v{nullptr, P->e32, P->r32, P->p32, P->ap32};
+  SolveScalars* si = P->sc_in;
+  auto pre = [&](cudaGraphConditionalHandle c) {
+    ProfScope ps(kKOther, s);
+    k_dc_to_inner<<<ln.grid, ln.block, 0, s>>>(l0.L, P->r, sc, P->r32, P->e32, si, ln.kchunk, rb, c);
+    OFB_LAUNCH_CHECK("k_dc_to_inner");
+  };
+  auto body = [&](cudaGraphConditionalHandle c) { enqueue_body<T, float>(P, v, si, rb, s, c); };
+  auto post = [&]() {
+    ProfScope ps(kKUpdateXr, s);
+    k_dc_update_x<<<ln.grid, ln.block, 0, s>>>(l0.L, P->x, P->e32, sc, si, ln.kchunk, rb);
+    k_dc_residual<<<ln.grid, ln.block, 0, s>>>(l0.op, P->b, P->x, P->r, sc, si, ln.kchunk, rb);
+    OFB_LAUNCH_CHECK("defect correction update");
+  };
+  const bool use_graph = P->use_graph && !prof_enabled();
+  long long inner_runs = 0;
+  while(host->cont) {
+    if(use_graph) {
+      if(P->exec == nullptr) P->exec = build_loop_graph(P, s, pre, body, &P->graph);
+      OFB_CHECK(cudaGraphLaunch(P->exec, s));
+      post();
+    } else {
+      pre(0);
+      SolveScalars hi{};
+      OFB_CHECK(cudaMemcpyAsync(&hi, si, sizeof(SolveScalars), cudaMemcpyDeviceToHost, s));
+      OFB_CHECK(cudaStreamSynchronize(s));
+      prof_collect();
+      while(hi.cont) {
+        body(0);
+        OFB_CHECK(cudaMemcpyAsync(&hi, si, sizeof(SolveScalars), cudaMemcpyDeviceToHost, s));
+        OFB_CHECK(cudaStreamSynchronize(s));
+        prof_collect();
+      }
+      post();
+    }
+    OFB_CHECK(cudaMemcpyAsync(host, sc, sizeof(SolveScalars), cudaMemcpyDeviceToHost, s));
+    OFB_CHECK(cudaStreamSynchronize(s));
+    if(use_graph) {
+      prof_add_counts(P->pre_counts, 1);
+      prof_add_counts(P->body_counts, host->body_runs - inner_runs);
+      inner_runs = host->body_runs;
+    }
+    prof_collect();
+  }
+  if(history != nullptr && history_cap > 0) {
+    const int n = std::min(history_cap, std::min(host->outer + 1, P->hist_cap));
+    OFB_CHECK(cudaMemcpy(history, P->hist, sizeof(double) * n, cudaMemcpyDeviceToHost));
+  }
+}
+
 }  // namespace
 
 void poisson_solve(PoissonPlan* P, int max_iterations, double tolerance, SolveScalars* sc_dev,
                    SolveScalars* sc_host, RedBuf rb, cudaStream_t s, double* history,
                    int history_cap) {
   if(P->precision == 1)
-    solve_impl<float>(P, max_iterations, tolerance, sc_dev, sc_host, rb, s, history, history_cap);
+    solve_dc<float>(P, max_iterations, tolerance, sc_dev, sc_host, rb, s, history, history_cap);
   else
     solve_impl<double>(P, max_iterations, tolerance, sc_dev, sc_host, rb, s, history, history_cap);
 }

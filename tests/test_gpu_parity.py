@@ -227,3 +227,29 @@ def test_poisson_nonconvergence_reports_like_reference(sb, oracle):
     st = ctx.download_state()
     assert st["metrics"]["step"] == 0  # the state is left at the last completed step
     assert np.array_equal(st["u"], s0.u)
+
+
+@pytest.mark.parametrize("n", [(32, 32, 32), (64, 32, 16), (48, 40, 8)])
+def test_mixed_precision_matches_fp64(sb, oracle, n):
+    """OF_MIXED (FP32 inner MG-PCG inside FP64 defect correction) converges to
+    the same relative residual as the FP64 path, so the states agree to the
+    solve tolerance (1e-12): checked at 1e-9 relative after 8 steps, and the
+    mixed state against the oracle at the same bound."""
+    cfg = po.steps_config(*n, 0.01, 0.5, 8, 1e-12)
+    g = oracle.tg_grid(cfg)
+    s0 = oracle.tg_init(cfg, 0)
+    outs = {}
+    for prec in (sb.OF_FP64, sb.OF_MIXED):
+        ctx = sb.Context(to_gpu_grid(g), to_gpu_bc(oracle.tg_bc(cfg)), precision=prec)
+        ctx.upload_state(s0.u, s0.v, s0.w, s0.adv_u, s0.adv_v, s0.adv_w, s0.p, 0, s0.metrics)
+        prm = sb.step_params(cfg.viscosity, oracle.tg_dt(cfg), cfg.poisson_max_iterations,
+                             cfg.poisson_tolerance)
+        m = ctx.run_steps(prm, 8)
+        outs[prec] = (ctx.download_state(), m)
+        ctx.close()
+    (a, ma), (b, mb) = outs[sb.OF_FP64], outs[sb.OF_MIXED]
+    assert mb["pressure_relative_residual"] <= 1e-12
+    ref = oracle.tg_steps(cfg, 8, s0.copy())
+    for name in ("u", "v", "w"):
+        assert rel_maxdiff(b[name], a[name]) <= 1e-9, name
+        assert rel_maxdiff(b[name], getattr(ref, name)) <= 1e-9, name
