@@ -1893,7 +1893,7 @@ void solve_impl(PoissonPlan* P, int max_iterations, double tolerance, SolveScala
 // residual scaled to unit RMS, to a relative residual of kInnerTol.  The
 // reported iteration count is the total number of inner iterations.
 // ---------------------------------------------------------------------------
-constexpr double kInnerTol = 1.0e-5;
+constexpr double kInnerTol = 1.0e-4;
 constexpr int kInnerMaxIt = 60;
 
 template <typename T>
