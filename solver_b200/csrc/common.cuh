@@ -248,6 +248,11 @@ struct CudaError : std::runtime_error {
   using std::runtime_error::runtime_error;
 };
 
+// A bounded device-side wait gave up (reported as OF_TIMEOUT).
+struct TimeoutError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
 inline void check_cuda(cudaError_t e, const char* what) {
   if(e != cudaSuccess) {
     throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));

@@ -37,6 +37,9 @@ of_status guarded(Fn&& fn) {
   } catch(const ofb::CudaError& e) {
     g_last_error = e.what();
     return OF_CUDA_ERROR;
+  } catch(const ofb::TimeoutError& e) {
+    g_last_error = e.what();
+    return OF_TIMEOUT;
   } catch(const std::invalid_argument& e) {
     g_last_error = e.what();
     return OF_INVALID_ARGUMENT;

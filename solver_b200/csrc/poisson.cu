@@ -21,6 +21,7 @@
 // arithmetic inside the FP64 CG loop).
 #include "kernels.hpp"
 #include "vstencil.cuh"
+#include "tma.cuh"
 
 #include <cmath>
 #include <cstdlib>
@@ -730,6 +731,703 @@ __global__ void k_coarse_solve(int n, const int* __restrict__ swaps, const doubl
 }
 
 // ---------------------------------------------------------------------------
+// Plane-pipelined stencil kernels.  A block owns a tile of whole rows (all nx
+// cells, TY = 1024 / nx rows) and a chunk of k planes.  One thread stages each
+// plane of the operand -- the tile rows plus the two neighbour rows, fetched at
+// their boundary images (periodic wrap or the mirrored row) -- and of the
+// rhs into a ring of kTSlots shared-memory slots with TMA, kTSlots - 2 planes
+// ahead of the compute; an mbarrier per slot carries the arrival.  Each
+// thread owns four consecutive cells of one row: their z-neighbours come from
+// a register queue, the in-plane neighbours from the staged plane.  Boundary
+// signs (Dirichlet mirrors) and mean shifts are applied on read.  Used where
+// nx is 64, 128 or 256 and TY divides ny.
+// ---------------------------------------------------------------------------
+constexpr int kTSlots = 5;
+constexpr int kTThreads = 256;
+
+__host__ __device__ inline size_t tround(size_t b) { return (b + 127) / 128 * 128; }
+
+template <typename T, typename B>
+__host__ __device__ inline size_t tslot_bytes(int nx) {
+  const int ty = 1024 / nx;
+  return tround(static_cast<size_t>(ty + 2) * nx * sizeof(T)) + tround(static_cast<size_t>(ty) * nx * sizeof(B));
+}
+
+template <typename T, typename B>
+__host__ __device__ inline size_t tprolong_bytes(int nx) {
+  const int ty = 1024 / nx;
+  return tround(static_cast<size_t>(ty + 2) * nx * sizeof(T)) + tround(static_cast<size_t>(ty) * nx * sizeof(B)) +
+         tround(static_cast<size_t>(ty / 2 + 2) * (nx / 2) * sizeof(T));
+}
+
+template <typename A, typename S>
+__device__ __forceinline__ void tload4(const S* p, A (&v)[4]) {
+  if constexpr(std::is_same_v<S, double>) {
+    const double2 a = *reinterpret_cast<const double2*>(p);
+    const double2 b = *reinterpret_cast<const double2*>(p + 2);
+    v[0] = A(a.x);
+    v[1] = A(a.y);
+    v[2] = A(b.x);
+    v[3] = A(b.y);
+  } else {
+    const float4 a = *reinterpret_cast<const float4*>(p);
+    v[0] = A(a.x);
+    v[1] = A(a.y);
+    v[2] = A(a.z);
+    v[3] = A(a.w);
+  }
+}
+
+template <typename S, typename A>
+__device__ __forceinline__ void tstore4(S* p, const A (&v)[4]) {
+  if constexpr(std::is_same_v<S, double>) {
+    *reinterpret_cast<double2*>(p) = make_double2(double(v[0]), double(v[1]));
+    *reinterpret_cast<double2*>(p + 2) = make_double2(double(v[2]), double(v[3]));
+  } else {
+    *reinterpret_cast<float4*>(p) = make_float4(float(v[0]), float(v[1]), float(v[2]), float(v[3]));
+  }
+}
+
+// Persistent schedule of the plane pipeline: the tile-planes (tile, k) of a
+// level, k fastest, are split into gridDim.x contiguous ranges of equal length
+// (within one); a block walks its range as segments (one per tile it touches)
+// and streams each segment's planes k_begin - 1 .. k_end through one ring, so
+// the pipeline is filled once per block and no block waits for a tail wave.
+constexpr int kTMaxSeg = 8;
+
+struct TSeg {
+  int tile, kb, ke, lbase;  // planes [kb, ke) of `tile`; first load index
+};
+
+__device__ __forceinline__ int tsegments(int tiles, int nz, TSeg (&seg)[kTMaxSeg], int& nload) {
+  const long long total = static_cast<long long>(tiles) * nz;
+  const long long f0 = total * blockIdx.x / gridDim.x;
+  const long long f1 = total * (blockIdx.x + 1) / gridDim.x;
+  int ns = 0;
+  nload = 0;
+  for(long long f = f0; f < f1 && ns < kTMaxSeg;) {
+    const int tile = static_cast<int>(f / nz);
+    const int kb = static_cast<int>(f % nz);
+    const int ke = static_cast<int>(min(static_cast<long long>(nz), kb + (f1 - f)));
+    seg[ns] = TSeg{tile, kb, ke, nload};
+    nload += ke - kb + 2;
+    f += ke - kb;
+    ++ns;
+  }
+  return ns;
+}
+
+// Jacobi sweep (smooth_jacobi, linsolve/poisson_solver.cpp:569-595) on the
+// plane pipeline: out = x + omega (b - sb - A x) / D with x = in - s_in;
+// records mean(out) (ls->sx) and, on the finest level, r.z (sc).  Same
+// contract as k_vsmooth.  CPT cells per thread (4 or 2), 1024 / CPT threads.
+template <typename T, typename B, int CPT>
+__global__ void __launch_bounds__(1024 / CPT)
+    k_tsmooth(OpInfo o, const __grid_constant__ CUtensorMap um, const __grid_constant__ CUtensorMap uh,
+              const __grid_constant__ CUtensorMap bm, const double* sb_ptr, const double* sin_ptr,
+              T* __restrict__ out, LevelScalars* ls, int zm, SolveScalars* sc, RedBuf rb, int* fault) {
+  using A = T;
+  constexpr int D = kTSlots;
+  extern __shared__ __align__(128) unsigned char tsm[];
+  __shared__ uint64_t bars[D];
+  __shared__ double invd_s[64];
+  const int NX = o.L.nx, NY = o.L.ny, NZ = o.L.nz;
+  const int TY = 1024 / NX;
+  const int tpr = NX / CPT;
+  const int r = threadIdx.x / tpr;
+  const int i0 = (threadIdx.x % tpr) * CPT;
+  const size_t ubytes = tround(static_cast<size_t>(TY + 2) * NX * sizeof(T));
+  const size_t sbytes = tslot_bytes<T, B>(NX);
+  const uint32_t tx_bytes = static_cast<uint32_t>((TY + 2) * NX * sizeof(T) + TY * NX * sizeof(B));
+  auto uslot = [&](int s) { return reinterpret_cast<T*>(tsm + s * sbytes); };
+  auto bslot = [&](int s) { return reinterpret_cast<B*>(tsm + s * sbytes + ubytes); };
+  TSeg seg[kTMaxSeg];
+  int nload = 0;
+  const int nseg = tsegments(NY / TY, NZ, seg, nload);
+  // producer (thread 0): load l -> its segment's tile and plane image
+  auto issue = [&](int l) {
+    int q = 0;
+    while(q + 1 < nseg && seg[q + 1].lbase <= l) ++q;
+    const int j0 = seg[q].tile * TY;
+    int jm, jp;
+    double sg;
+    nb_lo(j0, NY, o.periodic[1], o.dir_lo[1], jm, sg);
+    nb_hi(j0 + TY - 1, NY, o.periodic[1], o.dir_hi[1], jp, sg);
+    const int kz = vst::zrow(seg[q].kb - 1 + (l - seg[q].lbase), NZ, o.periodic[2], o.dir_lo[2],
+                             o.dir_hi[2], sg);
+    const int sl = l % D;
+    tma::mbar_arrive_expect_tx(&bars[sl], tx_bytes);
+    tma::load_3d(uslot(sl) + NX, &um, &bars[sl], 0, j0, kz);
+    tma::load_3d(uslot(sl), &uh, &bars[sl], 0, jm, kz);
+    tma::load_3d(uslot(sl) + (TY + 1) * NX, &uh, &bars[sl], 0, jp, kz);
+    tma::load_3d(bslot(sl), &bm, &bars[sl], 0, j0, kz);
+  };
+  if(threadIdx.x == 0) {
+    for(int sl = 0; sl < D; ++sl) tma::mbar_init(&bars[sl], 1);
+    tma::fence_barrier_init();
+  }
+  if(threadIdx.x < 64) invd_s[threadIdx.x] = o.invd[threadIdx.x];
+  __syncthreads();
+  int next = 0;  // next load to issue (meaningful on thread 0)
+  if(threadIdx.x == 0)
+    while(next < nload && next < D) issue(next++);
+  const double sb = *sb_ptr;
+  const A sin = A(*sin_ptr);
+  const A om = A(kOmega);
+  const A ix = A(o.inv2[0]), iy = A(o.inv2[1]), iz = A(o.inv2[2]);
+  auto ldrow = [&](const T* p, A (&v)[CPT]) {
+    if constexpr(CPT == 4) {
+      tload4<A>(p, v);
+    } else if constexpr(std::is_same_v<T, double>) {
+      const double2 a = *reinterpret_cast<const double2*>(p);
+      v[0] = A(a.x);
+      v[1] = A(a.y);
+    } else {
+      const float2 a = *reinterpret_cast<const float2*>(p);
+      v[0] = A(a.x);
+      v[1] = A(a.y);
+    }
+  };
+  double acc[2] = {0.0, 0.0};
+  int xl, xr;
+  double sxl, sxr;
+  nb_lo(i0, NX, o.periodic[0], o.dir_lo[0], xl, sxl);
+  nb_hi(i0 + CPT - 1, NX, o.periodic[0], o.dir_hi[0], xr, sxr);
+  for(int q = 0; q < nseg; ++q) {
+    const TSeg sg = seg[q];
+    const int j0 = sg.tile * TY;
+    const int j = j0 + r;
+    int jm, jp;
+    double sylo, syhi;
+    nb_lo(j0, NY, o.periodic[1], o.dir_lo[1], jm, sylo);
+    nb_hi(j0 + TY - 1, NY, o.periodic[1], o.dir_hi[1], jp, syhi);
+    int cls[CPT];
+#pragma unroll
+    for(int t = 0; t < CPT; ++t) cls[t] = axis_class(i0 + t, NX) + 4 * axis_class(j, NY);
+    auto own = [&](int l, A (&v)[CPT]) {
+      tma::mbar_wait(&bars[l % D], (l / D) & 1, fault, 1);
+      double zs;
+      vst::zrow(sg.kb - 1 + (l - sg.lbase), NZ, o.periodic[2], o.dir_lo[2], o.dir_hi[2], zs);
+      ldrow(uslot(l % D) + (r + 1) * NX + i0, v);
+#pragma unroll
+      for(int t = 0; t < CPT; ++t) v[t] = A(zs) * (v[t] - sin);
+    };
+    A below[CPT], cen[CPT], above[CPT];
+    own(sg.lbase, below);
+    own(sg.lbase + 1, cen);
+    __syncthreads();
+    for(int k = sg.kb; k < sg.ke; ++k) {
+      const int c = sg.lbase + 1 + (k - sg.kb);  // load of plane k
+      if(threadIdx.x == 0) {
+        tma::fence_proxy_async();
+        while(next < nload && next <= c - 1 + D) issue(next++);
+      }
+      own(c + 1, above);
+      const T* pk = uslot(c % D);
+      const B* bk = bslot(c % D);
+      A dn[CPT], up[CPT];
+      ldrow(pk + r * NX + i0, dn);
+      ldrow(pk + (r + 2) * NX + i0, up);
+      const A sd = r == 0 ? A(sylo) : A(1), su = r == TY - 1 ? A(syhi) : A(1);
+#pragma unroll
+      for(int t = 0; t < CPT; ++t) {
+        dn[t] = sd * (dn[t] - sin);
+        up[t] = su * (up[t] - sin);
+      }
+      const A left = A(sxl) * (pk[(r + 1) * NX + xl] - sin);
+      const A right = A(sxr) * (pk[(r + 1) * NX + xr] - sin);
+      double bq[CPT];
+      if constexpr(CPT == 4) {
+        tload4<double>(bk + r * NX + i0, bq);
+      } else {
+#pragma unroll
+        for(int t = 0; t < CPT; ++t) bq[t] = double(bk[r * NX + i0 + t]);
+      }
+      const int cz = 16 * axis_class(k, NZ);
+      A v[CPT];
+#pragma unroll
+      for(int t = 0; t < CPT; ++t) {
+        const double bd = bq[t] - sb;
+        const A l = t > 0 ? cen[t - 1] : left;
+        const A rr = t < CPT - 1 ? cen[t + 1] : right;
+        const A two_c = A(2) * cen[t];
+        const A ax = -(rr - two_c + l) * ix - (up[t] - two_c + dn[t]) * iy - (above[t] - two_c + below[t]) * iz;
+        v[t] = cen[t] + om * (A(bd) - ax) * A(invd_s[cls[t] + cz]);
+        acc[0] += double(v[t]);
+        acc[1] += bd * double(v[t]);
+      }
+      if constexpr(CPT == 4) {
+        tstore4<T>(out + o.L.idx(i0, j, k), v);
+      } else if constexpr(std::is_same_v<T, double>) {
+        *reinterpret_cast<double2*>(out + o.L.idx(i0, j, k)) = make_double2(v[0], v[1]);
+      } else {
+        *reinterpret_cast<float2*>(out + o.L.idx(i0, j, k)) = make_float2(v[0], v[1]);
+      }
+#pragma unroll
+      for(int t = 0; t < CPT; ++t) {
+        below[t] = cen[t];
+        cen[t] = above[t];
+      }
+      __syncthreads();
+    }
+  }
+  const bool mx[2] = {false, false};
+  const int n = o.L.count();
+  reduce_finish<2>(acc, mx, rb, [=](const Sums<2>& st) {
+    const double mean = zm ? st.v[0] / n : 0.0;
+    ls->sx = mean;
+    ls->sum_x = st.v[0];
+    if(sc != nullptr) {
+      const double rz_new = st.v[1] - mean * (sc->sum_r - sc->n * sc->sr);
+      if(sc->first) {
+        sc->rz = rz_new;
+      } else {
+        sc->beta = rz_new / sc->rz;
+        sc->rz = rz_new;
+      }
+    }
+  });
+}
+
+// Both pre-smoothing sweeps from a zero correction on the plane pipeline
+// (same contract as k_vsmooth_pre): the staged operand is b itself, and the
+// first sweep's a = omega (b - sb) / D is formed on read for every stencil
+// point, with the diagonal of the point's boundary image.
+template <typename T, typename B, int CPT>
+__global__ void __launch_bounds__(1024 / CPT)
+    k_tsmooth_pre(OpInfo o, const __grid_constant__ CUtensorMap bm, const __grid_constant__ CUtensorMap bh,
+                  const double* sb_ptr, T* __restrict__ out, LevelScalars* ls, int zm, RedBuf rb,
+                  int* fault) {
+  using A = T;
+  constexpr int D = kTSlots;
+  extern __shared__ __align__(128) unsigned char tsm[];
+  __shared__ uint64_t bars[D];
+  __shared__ double invd_s[64];
+  const int NX = o.L.nx, NY = o.L.ny, NZ = o.L.nz;
+  const int TY = 1024 / NX;
+  const int tpr = NX / CPT;
+  const int r = threadIdx.x / tpr;
+  const int i0 = (threadIdx.x % tpr) * CPT;
+  const size_t sbytes = tround(static_cast<size_t>(TY + 2) * NX * sizeof(B));
+  const uint32_t tx_bytes = static_cast<uint32_t>((TY + 2) * NX * sizeof(B));
+  auto slot = [&](int s) { return reinterpret_cast<B*>(tsm + s * sbytes); };
+  TSeg seg[kTMaxSeg];
+  int nload = 0;
+  const int nseg = tsegments(NY / TY, NZ, seg, nload);
+  auto issue = [&](int l) {
+    int q = 0;
+    while(q + 1 < nseg && seg[q + 1].lbase <= l) ++q;
+    const int j0 = seg[q].tile * TY;
+    int jm, jp;
+    double sg;
+    nb_lo(j0, NY, o.periodic[1], o.dir_lo[1], jm, sg);
+    nb_hi(j0 + TY - 1, NY, o.periodic[1], o.dir_hi[1], jp, sg);
+    const int kz = vst::zrow(seg[q].kb - 1 + (l - seg[q].lbase), NZ, o.periodic[2], o.dir_lo[2],
+                             o.dir_hi[2], sg);
+    const int sl = l % D;
+    tma::mbar_arrive_expect_tx(&bars[sl], tx_bytes);
+    tma::load_3d(slot(sl) + NX, &bm, &bars[sl], 0, j0, kz);
+    tma::load_3d(slot(sl), &bh, &bars[sl], 0, jm, kz);
+    tma::load_3d(slot(sl) + (TY + 1) * NX, &bh, &bars[sl], 0, jp, kz);
+  };
+  if(threadIdx.x == 0) {
+    for(int sl = 0; sl < D; ++sl) tma::mbar_init(&bars[sl], 1);
+    tma::fence_barrier_init();
+  }
+  if(threadIdx.x < 64) invd_s[threadIdx.x] = o.invd[threadIdx.x];
+  __syncthreads();
+  int next = 0;
+  if(threadIdx.x == 0)
+    while(next < nload && next < D) issue(next++);
+  const double sb = *sb_ptr;
+  const A om = A(kOmega);
+  const A ix = A(o.inv2[0]), iy = A(o.inv2[1]), iz = A(o.inv2[2]);
+  auto ldrow = [&](const B* p, double (&v)[CPT]) {
+    if constexpr(CPT == 4) {
+      tload4<double>(p, v);
+    } else {
+#pragma unroll
+      for(int t = 0; t < CPT; ++t) v[t] = double(p[t]);
+    }
+  };
+  double acc[1] = {0.0};
+  int xl, xr;
+  double sxl, sxr;
+  nb_lo(i0, NX, o.periodic[0], o.dir_lo[0], xl, sxl);
+  nb_hi(i0 + CPT - 1, NX, o.periodic[0], o.dir_hi[0], xr, sxr);
+  for(int q = 0; q < nseg; ++q) {
+    const TSeg sg = seg[q];
+    const int j0 = sg.tile * TY;
+    const int j = j0 + r;
+    int jm, jp;
+    double sylo, syhi;
+    nb_lo(j0, NY, o.periodic[1], o.dir_lo[1], jm, sylo);
+    nb_hi(j0 + TY - 1, NY, o.periodic[1], o.dir_hi[1], jp, syhi);
+    // boundary classes (x + 4 y) of the own cells and of their in-plane neighbours' images
+    const int jd = r == 0 ? jm : j - 1, ju = r == TY - 1 ? jp : j + 1;
+    const A sd = r == 0 ? A(sylo) : A(1), su = r == TY - 1 ? A(syhi) : A(1);
+    int cown[CPT], cdn[CPT], cup[CPT];
+#pragma unroll
+    for(int t = 0; t < CPT; ++t) {
+      const int cx = axis_class(i0 + t, NX);
+      cown[t] = cx + 4 * axis_class(j, NY);
+      cdn[t] = cx + 4 * axis_class(jd, NY);
+      cup[t] = cx + 4 * axis_class(ju, NY);
+    }
+    const int cl = axis_class(xl, NX) + 4 * axis_class(j, NY);
+    const int cr = axis_class(xr, NX) + 4 * axis_class(j, NY);
+    // a of the own cells at load l (its plane's image and sign)
+    auto own = [&](int l, A (&v)[CPT]) {
+      tma::mbar_wait(&bars[l % D], (l / D) & 1, fault, 1);
+      double zs;
+      const int kz = vst::zrow(sg.kb - 1 + (l - sg.lbase), NZ, o.periodic[2], o.dir_lo[2], o.dir_hi[2], zs);
+      const int cz = 16 * axis_class(kz, NZ);
+      double b[CPT];
+      ldrow(slot(l % D) + (r + 1) * NX + i0, b);
+#pragma unroll
+      for(int t = 0; t < CPT; ++t) v[t] = A(zs) * om * A(b[t] - sb) * A(invd_s[cown[t] + cz]);
+    };
+    A below[CPT], cen[CPT], above[CPT];
+    own(sg.lbase, below);
+    own(sg.lbase + 1, cen);
+    __syncthreads();
+    for(int k = sg.kb; k < sg.ke; ++k) {
+      const int c = sg.lbase + 1 + (k - sg.kb);
+      if(threadIdx.x == 0) {
+        tma::fence_proxy_async();
+        while(next < nload && next <= c - 1 + D) issue(next++);
+      }
+      own(c + 1, above);
+      const B* pk = slot(c % D);
+      const int cz = 16 * axis_class(k, NZ);
+      double bd[CPT], bu[CPT], bc[CPT];
+      ldrow(pk + r * NX + i0, bd);
+      ldrow(pk + (r + 2) * NX + i0, bu);
+      ldrow(pk + (r + 1) * NX + i0, bc);
+      A dn[CPT], up[CPT];
+#pragma unroll
+      for(int t = 0; t < CPT; ++t) {
+        dn[t] = sd * om * A(bd[t] - sb) * A(invd_s[cdn[t] + cz]);
+        up[t] = su * om * A(bu[t] - sb) * A(invd_s[cup[t] + cz]);
+      }
+      const A left = A(sxl) * om * A(double(pk[(r + 1) * NX + xl]) - sb) * A(invd_s[cl + cz]);
+      const A right = A(sxr) * om * A(double(pk[(r + 1) * NX + xr]) - sb) * A(invd_s[cr + cz]);
+      A v[CPT];
+#pragma unroll
+      for(int t = 0; t < CPT; ++t) {
+        const A l = t > 0 ? cen[t - 1] : left;
+        const A rr = t < CPT - 1 ? cen[t + 1] : right;
+        const A two_c = A(2) * cen[t];
+        const A ax = -(rr - two_c + l) * ix - (up[t] - two_c + dn[t]) * iy - (above[t] - two_c + below[t]) * iz;
+        v[t] = cen[t] + om * (A(bc[t] - sb) - ax) * A(invd_s[cown[t] + cz]);
+        acc[0] += double(v[t]);
+      }
+      if constexpr(CPT == 4) {
+        tstore4<T>(out + o.L.idx(i0, j, k), v);
+      } else if constexpr(std::is_same_v<T, double>) {
+        *reinterpret_cast<double2*>(out + o.L.idx(i0, j, k)) = make_double2(v[0], v[1]);
+      } else {
+        *reinterpret_cast<float2*>(out + o.L.idx(i0, j, k)) = make_float2(v[0], v[1]);
+      }
+#pragma unroll
+      for(int t = 0; t < CPT; ++t) {
+        below[t] = cen[t];
+        cen[t] = above[t];
+      }
+      __syncthreads();
+    }
+  }
+  const bool mx[1] = {false};
+  const int n = o.L.count();
+  reduce_finish<1>(acc, mx, rb, [=](const Sums<1>& st) {
+    ls->sx = zm ? st.v[0] / n : 0.0;
+    ls->sum_x = st.v[0];
+  });
+}
+
+// Prolongation + first post-smoothing sweep on the plane pipeline (same
+// contract as k_vprolong_smooth, 2x2x2 coarsening): the staged operand is the
+// level's correction x and the coarse correction ec (parent rows and the
+// parents of the halo rows), combined on read as (x - sx) + (ec - sec).
+template <typename T, typename B, int CPT, int D>
+__global__ void __launch_bounds__(1024 / CPT)
+    k_tprolong(OpInfo o, const __grid_constant__ CUtensorMap xm, const __grid_constant__ CUtensorMap xh,
+               const __grid_constant__ CUtensorMap bm, const __grid_constant__ CUtensorMap em,
+               const __grid_constant__ CUtensorMap eh, const double* sb_ptr, const double* sin_ptr,
+               const double* sec_ptr, T* __restrict__ out, LevelScalars* ls, int zm, RedBuf rb,
+               int* fault) {
+  using A = T;
+  extern __shared__ __align__(128) unsigned char tsm[];
+  __shared__ uint64_t bars[D];
+  __shared__ double invd_s[64];
+  const int NX = o.L.nx, NY = o.L.ny, NZ = o.L.nz;
+  const int NXc = NX / 2, NZc = NZ / 2;
+  const int TY = 1024 / NX;
+  const int TYc = TY / 2;
+  const int tpr = NX / CPT;
+  const int r = threadIdx.x / tpr;
+  const int i0 = (threadIdx.x % tpr) * CPT;
+  const size_t xbytes = tround(static_cast<size_t>(TY + 2) * NX * sizeof(T));
+  const size_t bbytes = tround(static_cast<size_t>(TY) * NX * sizeof(B));
+  const size_t ebytes = tround(static_cast<size_t>(TYc + 2) * NXc * sizeof(T));
+  const size_t sbytes = xbytes + bbytes + ebytes;
+  const uint32_t tx_bytes = static_cast<uint32_t>((TY + 2) * NX * sizeof(T) + TY * NX * sizeof(B) +
+                                                  (TYc + 2) * NXc * sizeof(T));
+  auto xslot = [&](int s) { return reinterpret_cast<T*>(tsm + s * sbytes); };
+  auto bslot = [&](int s) { return reinterpret_cast<B*>(tsm + s * sbytes + xbytes); };
+  auto eslot = [&](int s) { return reinterpret_cast<T*>(tsm + s * sbytes + xbytes + bbytes); };
+  TSeg seg[kTMaxSeg];
+  int nload = 0;
+  const int nseg = tsegments(NY / TY, NZ, seg, nload);
+  auto issue = [&](int l) {
+    int q = 0;
+    while(q + 1 < nseg && seg[q + 1].lbase <= l) ++q;
+    const int j0 = seg[q].tile * TY;
+    int jm, jp;
+    double sg;
+    nb_lo(j0, NY, o.periodic[1], o.dir_lo[1], jm, sg);
+    nb_hi(j0 + TY - 1, NY, o.periodic[1], o.dir_hi[1], jp, sg);
+    const int kz = vst::zrow(seg[q].kb - 1 + (l - seg[q].lbase), NZ, o.periodic[2], o.dir_lo[2],
+                             o.dir_hi[2], sg);
+    const int sl = l % D;
+    tma::mbar_arrive_expect_tx(&bars[sl], tx_bytes);
+    tma::load_3d(xslot(sl) + NX, &xm, &bars[sl], 0, j0, kz);
+    tma::load_3d(xslot(sl), &xh, &bars[sl], 0, jm, kz);
+    tma::load_3d(xslot(sl) + (TY + 1) * NX, &xh, &bars[sl], 0, jp, kz);
+    tma::load_3d(bslot(sl), &bm, &bars[sl], 0, j0, kz);
+    tma::load_3d(eslot(sl) + NXc, &em, &bars[sl], 0, j0 >> 1, kz >> 1);
+    tma::load_3d(eslot(sl), &eh, &bars[sl], 0, jm >> 1, kz >> 1);
+    tma::load_3d(eslot(sl) + (TYc + 1) * NXc, &eh, &bars[sl], 0, jp >> 1, kz >> 1);
+  };
+  (void)NZc;
+  if(threadIdx.x == 0) {
+    for(int sl = 0; sl < D; ++sl) tma::mbar_init(&bars[sl], 1);
+    tma::fence_barrier_init();
+  }
+  if(threadIdx.x < 64) invd_s[threadIdx.x] = o.invd[threadIdx.x];
+  __syncthreads();
+  int next = 0;
+  if(threadIdx.x == 0)
+    while(next < nload && next < D) issue(next++);
+  const double sb = *sb_ptr;
+  const A sin = A(*sin_ptr);
+  const A sec = A(*sec_ptr);
+  const A om = A(kOmega);
+  const A ix = A(o.inv2[0]), iy = A(o.inv2[1]), iz = A(o.inv2[2]);
+  // fine slot row (0 .. TY+1) -> coarse slot row of its parent
+  auto crow = [&](int fr) { return fr == 0 ? 0 : (fr == TY + 1 ? TYc + 1 : ((fr - 1) >> 1) + 1); };
+  // combined operand of the CPT cells at fine slot row fr (shifted, unsigned)
+  auto operand = [&](const T* xs, const T* es, int fr, A (&v)[CPT]) {
+    A xv[CPT];
+    tload4<A>(xs + fr * NX + i0, xv);
+    const T* erow = es + crow(fr) * NXc + (i0 >> 1);
+    const A e0 = A(erow[0]) - sec, e1 = A(erow[1]) - sec;
+    v[0] = (xv[0] - sin) + e0;
+    v[1] = (xv[1] - sin) + e0;
+    v[2] = (xv[2] - sin) + e1;
+    v[3] = (xv[3] - sin) + e1;
+  };
+  double acc[1] = {0.0};
+  int xl, xr;
+  double sxl, sxr;
+  nb_lo(i0, NX, o.periodic[0], o.dir_lo[0], xl, sxl);
+  nb_hi(i0 + CPT - 1, NX, o.periodic[0], o.dir_hi[0], xr, sxr);
+  for(int q = 0; q < nseg; ++q) {
+    const TSeg sg = seg[q];
+    const int j0 = sg.tile * TY;
+    const int j = j0 + r;
+    int jm, jp;
+    double sylo, syhi;
+    nb_lo(j0, NY, o.periodic[1], o.dir_lo[1], jm, sylo);
+    nb_hi(j0 + TY - 1, NY, o.periodic[1], o.dir_hi[1], jp, syhi);
+    int cls[CPT];
+#pragma unroll
+    for(int t = 0; t < CPT; ++t) cls[t] = axis_class(i0 + t, NX) + 4 * axis_class(j, NY);
+    auto own = [&](int l, A (&v)[CPT]) {
+      tma::mbar_wait(&bars[l % D], (l / D) & 1, fault, 1);
+      double zs;
+      vst::zrow(sg.kb - 1 + (l - sg.lbase), NZ, o.periodic[2], o.dir_lo[2], o.dir_hi[2], zs);
+      operand(xslot(l % D), eslot(l % D), r + 1, v);
+#pragma unroll
+      for(int t = 0; t < CPT; ++t) v[t] *= A(zs);
+    };
+    A below[CPT], cen[CPT], above[CPT];
+    own(sg.lbase, below);
+    own(sg.lbase + 1, cen);
+    __syncthreads();
+    for(int k = sg.kb; k < sg.ke; ++k) {
+      const int c = sg.lbase + 1 + (k - sg.kb);
+      if(threadIdx.x == 0) {
+        tma::fence_proxy_async();
+        while(next < nload && next <= c - 1 + D) issue(next++);
+      }
+      own(c + 1, above);
+      const T* xs = xslot(c % D);
+      const T* es = eslot(c % D);
+      const B* bk = bslot(c % D);
+      A dn[CPT], up[CPT];
+      operand(xs, es, r, dn);
+      operand(xs, es, r + 2, up);
+      const A sd = r == 0 ? A(sylo) : A(1), su = r == TY - 1 ? A(syhi) : A(1);
+#pragma unroll
+      for(int t = 0; t < CPT; ++t) {
+        dn[t] *= sd;
+        up[t] *= su;
+      }
+      const T* erow = es + crow(r + 1) * NXc;
+      const A left = A(sxl) * ((A(xs[(r + 1) * NX + xl]) - sin) + (A(erow[xl >> 1]) - sec));
+      const A right = A(sxr) * ((A(xs[(r + 1) * NX + xr]) - sin) + (A(erow[xr >> 1]) - sec));
+      double bq[CPT];
+      tload4<double>(bk + r * NX + i0, bq);
+      const int cz = 16 * axis_class(k, NZ);
+      A v[CPT];
+#pragma unroll
+      for(int t = 0; t < CPT; ++t) {
+        const A l = t > 0 ? cen[t - 1] : left;
+        const A rr = t < CPT - 1 ? cen[t + 1] : right;
+        const A two_c = A(2) * cen[t];
+        const A ax = -(rr - two_c + l) * ix - (up[t] - two_c + dn[t]) * iy - (above[t] - two_c + below[t]) * iz;
+        v[t] = cen[t] + om * (A(bq[t] - sb) - ax) * A(invd_s[cls[t] + cz]);
+        acc[0] += double(v[t]);
+      }
+      tstore4<T>(out + o.L.idx(i0, j, k), v);
+#pragma unroll
+      for(int t = 0; t < CPT; ++t) {
+        below[t] = cen[t];
+        cen[t] = above[t];
+      }
+      __syncthreads();
+    }
+  }
+  const bool mx[1] = {false};
+  const int n = o.L.count();
+  reduce_finish<1>(acc, mx, rb, [=](const Sums<1>& st) { ls->sa = zm ? st.v[0] / n : 0.0; });
+}
+
+// A p on the plane pipeline (same contract as k_vapply_ap).
+template <typename V, int CPT>
+__global__ void __launch_bounds__(1024 / CPT)
+    k_tap(OpInfo o, const __grid_constant__ CUtensorMap pm, const __grid_constant__ CUtensorMap ph,
+          V* __restrict__ ap, SolveScalars* sc, RedBuf rb, int* fault) {
+  constexpr int D = kTSlots;
+  extern __shared__ __align__(128) unsigned char tsm[];
+  __shared__ uint64_t bars[D];
+  const int NX = o.L.nx, NY = o.L.ny, NZ = o.L.nz;
+  const int TY = 1024 / NX;
+  const int tpr = NX / CPT;
+  const int r = threadIdx.x / tpr;
+  const int i0 = (threadIdx.x % tpr) * CPT;
+  const size_t sbytes = tround(static_cast<size_t>(TY + 2) * NX * sizeof(V));
+  const uint32_t tx_bytes = static_cast<uint32_t>((TY + 2) * NX * sizeof(V));
+  auto slot = [&](int s) { return reinterpret_cast<V*>(tsm + s * sbytes); };
+  TSeg seg[kTMaxSeg];
+  int nload = 0;
+  const int nseg = tsegments(NY / TY, NZ, seg, nload);
+  auto issue = [&](int l) {
+    int q = 0;
+    while(q + 1 < nseg && seg[q + 1].lbase <= l) ++q;
+    const int j0 = seg[q].tile * TY;
+    int jm, jp;
+    double sg;
+    nb_lo(j0, NY, o.periodic[1], o.dir_lo[1], jm, sg);
+    nb_hi(j0 + TY - 1, NY, o.periodic[1], o.dir_hi[1], jp, sg);
+    const int kz = vst::zrow(seg[q].kb - 1 + (l - seg[q].lbase), NZ, o.periodic[2], o.dir_lo[2],
+                             o.dir_hi[2], sg);
+    const int sl = l % D;
+    tma::mbar_arrive_expect_tx(&bars[sl], tx_bytes);
+    tma::load_3d(slot(sl) + NX, &pm, &bars[sl], 0, j0, kz);
+    tma::load_3d(slot(sl), &ph, &bars[sl], 0, jm, kz);
+    tma::load_3d(slot(sl) + (TY + 1) * NX, &ph, &bars[sl], 0, jp, kz);
+  };
+  if(threadIdx.x == 0) {
+    for(int sl = 0; sl < D; ++sl) tma::mbar_init(&bars[sl], 1);
+    tma::fence_barrier_init();
+  }
+  __syncthreads();
+  int next = 0;
+  if(threadIdx.x == 0)
+    while(next < nload && next < D) issue(next++);
+  const double sp = sc->sp;
+  const double ix = o.inv2[0], iy = o.inv2[1], iz = o.inv2[2];
+  double acc[3] = {0.0, 0.0, 0.0};
+  int xl, xr;
+  double sxl, sxr;
+  nb_lo(i0, NX, o.periodic[0], o.dir_lo[0], xl, sxl);
+  nb_hi(i0 + CPT - 1, NX, o.periodic[0], o.dir_hi[0], xr, sxr);
+  for(int q = 0; q < nseg; ++q) {
+    const TSeg sg = seg[q];
+    const int j0 = sg.tile * TY;
+    const int j = j0 + r;
+    int jm, jp;
+    double sylo, syhi;
+    nb_lo(j0, NY, o.periodic[1], o.dir_lo[1], jm, sylo);
+    nb_hi(j0 + TY - 1, NY, o.periodic[1], o.dir_hi[1], jp, syhi);
+    auto own = [&](int l, double (&v)[CPT]) {
+      tma::mbar_wait(&bars[l % D], (l / D) & 1, fault, 1);
+      double zs;
+      vst::zrow(sg.kb - 1 + (l - sg.lbase), NZ, o.periodic[2], o.dir_lo[2], o.dir_hi[2], zs);
+      tload4<double>(slot(l % D) + (r + 1) * NX + i0, v);
+#pragma unroll
+      for(int t = 0; t < CPT; ++t) v[t] = zs * (v[t] - sp);
+    };
+    double below[CPT], cen[CPT], above[CPT];
+    own(sg.lbase, below);
+    own(sg.lbase + 1, cen);
+    __syncthreads();
+    for(int k = sg.kb; k < sg.ke; ++k) {
+      const int c = sg.lbase + 1 + (k - sg.kb);
+      if(threadIdx.x == 0) {
+        tma::fence_proxy_async();
+        while(next < nload && next <= c - 1 + D) issue(next++);
+      }
+      own(c + 1, above);
+      const V* pk = slot(c % D);
+      double dn[CPT], up[CPT];
+      tload4<double>(pk + r * NX + i0, dn);
+      tload4<double>(pk + (r + 2) * NX + i0, up);
+      const double sd = r == 0 ? sylo : 1.0, su = r == TY - 1 ? syhi : 1.0;
+#pragma unroll
+      for(int t = 0; t < CPT; ++t) {
+        dn[t] = sd * (dn[t] - sp);
+        up[t] = su * (up[t] - sp);
+      }
+      const double left = sxl * (double(pk[(r + 1) * NX + xl]) - sp);
+      const double right = sxr * (double(pk[(r + 1) * NX + xr]) - sp);
+      double v[CPT];
+#pragma unroll
+      for(int t = 0; t < CPT; ++t) {
+        const double l = t > 0 ? cen[t - 1] : left;
+        const double rr = t < CPT - 1 ? cen[t + 1] : right;
+        const double two_c = 2.0 * cen[t];
+        v[t] = -(rr - two_c + l) * ix - (up[t] - two_c + dn[t]) * iy - (above[t] - two_c + below[t]) * iz;
+        acc[0] += v[t];
+        acc[1] += cen[t] * v[t];
+        acc[2] += cen[t];
+      }
+      tstore4<V>(ap + o.L.idx(i0, j, k), v);
+#pragma unroll
+      for(int t = 0; t < CPT; ++t) {
+        below[t] = cen[t];
+        cen[t] = above[t];
+      }
+      __syncthreads();
+    }
+  }
+  const bool mx[3] = {false, false, false};
+  reduce_finish<3>(acc, mx, rb, [=](const Sums<3>& st) {
+    const double sap = sc->zero_mean ? st.v[0] / sc->n : 0.0;
+    sc->sap = sap;
+    const double pap = st.v[1] - sap * st.v[2];
+    sc->pap = pap;
+    if(fabs(pap) < kSmallNumber) {
+      sc->stop = 1;
+    } else {
+      sc->alpha = sc->rz / pap;
+    }
+  });
+}
+
+// ---------------------------------------------------------------------------
 // The small end of the hierarchy in one block.  From the first level of at
 // most kTailMaxCells cells down to the coarsest, v_cycle (:597-633) runs in
 // one 1024-thread block with every level's rhs, correction and scratch in
@@ -738,9 +1436,9 @@ __global__ void k_coarse_solve(int n, const int* __restrict__ swaps, const doubl
 // by a block reduction.  One launch replaces five launches per level, each of
 // which was mostly launch latency and a dependent-load chain.
 // ---------------------------------------------------------------------------
-constexpr int kTailMaxCells = 4096;
+constexpr int kTailMaxCells = 512;
 constexpr int kTailMaxLevels = 12;
-constexpr int kTailThreads = 1024;
+constexpr int kTailThreads = 256;
 
 struct TailLevel {
   OpInfo op;
@@ -758,17 +1456,21 @@ struct TailArgs {
   int zm;
 };
 
-// Block-wide sum; every thread gets the same total (fixed order).
+// Block-wide sum; every thread gets the same total (fixed order).  red has
+// 33 entries: the warp partials and the total.
 __device__ __forceinline__ double tail_sum(double v, double* red) {
   v = warp_sum(v);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if(lane == 0) red[warp] = v;
   __syncthreads();
-  double s = 0.0;
-  const int nw = (blockDim.x + 31) >> 5;
-  for(int w = 0; w < nw; ++w) s += red[w];
+  if(warp == 0) {
+    const int nw = (blockDim.x + 31) >> 5;
+    double x = lane < nw ? red[lane] : 0.0;
+    x = warp_sum(x);
+    if(lane == 0) red[32] = x;
+  }
   __syncthreads();
-  return s;
+  return red[32];
 }
 
 __device__ __forceinline__ void tail_coords(const CLay& L, int q, int& i, int& j, int& k) {
@@ -806,7 +1508,7 @@ __global__ void __launch_bounds__(kTailThreads)
   using A = T;
   extern __shared__ __align__(16) unsigned char tail_smem[];
   A* sm = reinterpret_cast<A*>(tail_smem);
-  __shared__ double red[32];
+  __shared__ double red[33];
   const int tid = threadIdx.x, bd = blockDim.x;
   const int zm = a.zm;
   auto B = [&](int l) { return sm + a.lv[l].off; };
@@ -1256,6 +1958,11 @@ struct Level {
   void* b = nullptr;   // rhs (levels >= 1)
   double* invd = nullptr;
   int rx = 1, ry = 1, rz = 1;  // refinement ratio to the next coarser level
+  // plane-pipeline (TMA) maps: a (main rows, one halo row) and the rhs
+  bool tma = false;
+  CUtensorMap tm_am, tm_ah, tm_bm, tm_bh;
+  bool tma_prolong = false;  // 2x2x2 coarsening: correction x and the coarse result
+  CUtensorMap tm_xm, tm_xh, tm_em, tm_eh;
 };
 
 struct PoissonPlan {
@@ -1281,6 +1988,10 @@ struct PoissonPlan {
   // mixed path: inner (FP32) CG vectors and scalars
   float *r32 = nullptr, *e32 = nullptr, *p32 = nullptr, *ap32 = nullptr;
   SolveScalars* sc_in = nullptr;
+  int* fault = nullptr;  // device: a bounded wait in a plane-pipelined kernel gave up
+  int sms = 148;         // streaming multiprocessors of the plan's device
+  bool tma_ap = false;   // plane-pipelined A p on the finest level
+  CUtensorMap tm_pm, tm_ph;
   // levels tail_first.. run as one single-block launch (k_vcycle_tail)
   int tail_first = -1;
   TailArgs tail{};
@@ -1422,6 +2133,71 @@ void setup_tail(PoissonPlan* P, size_t tsz) {
   }
 }
 
+// Tensor maps of the plane-pipelined kernels for every level above the
+// single-block tail whose rows fit one TMA box (nx of 64, 128 or 256) and
+// whose row tiles divide ny.  ORCHARD_B200_NO_TMA=1 keeps the row kernels.
+bool tma_fits(const CLay& L) {
+  if(L.nx != 64 && L.nx != 128 && L.nx != 256) return false;
+  const int ty = 1024 / L.nx;
+  return L.ny % ty == 0 && L.nz >= 1;
+}
+
+void setup_tma(PoissonPlan* P, size_t tsz) {
+  const char* e = std::getenv("ORCHARD_B200_NO_TMA");
+  if(e != nullptr && e[0] == '1') return;
+  const int nl = static_cast<int>(P->levels.size());
+  const int last = P->tail_first >= 0 ? P->tail_first : nl - 1;
+  for(int l = 0; l < last; ++l) {
+    Level& lv = P->levels[l];
+    if(!tma_fits(lv.L)) continue;
+    const int ty = 1024 / lv.L.nx;
+    const int es = static_cast<int>(tsz);
+    lv.tm_am = tma::make_map_3d(lv.a, es, lv.L.nx, lv.L.ny, lv.L.nz, lv.L.nx, ty);
+    lv.tm_ah = tma::make_map_3d(lv.a, es, lv.L.nx, lv.L.ny, lv.L.nz, lv.L.nx, 1);
+    // the finest level's rhs is the CG residual: FP64, or FP32 on the mixed path
+    const void* bp = l > 0 ? lv.b : (P->precision == 1 ? static_cast<const void*>(P->r32) : P->r);
+    const int bes = l > 0 ? es : (P->precision == 1 ? 4 : 8);
+    lv.tm_bm = tma::make_map_3d(bp, bes, lv.L.nx, lv.L.ny, lv.L.nz, lv.L.nx, ty);
+    lv.tm_bh = tma::make_map_3d(bp, bes, lv.L.nx, lv.L.ny, lv.L.nz, lv.L.nx, 1);
+    lv.tma = true;
+    if(lv.rx == 2 && lv.ry == 2 && lv.rz == 2 && l + 1 < nl) {
+      const Level& cv = P->levels[l + 1];
+      lv.tm_xm = tma::make_map_3d(lv.x, es, lv.L.nx, lv.L.ny, lv.L.nz, lv.L.nx, ty);
+      lv.tm_xh = tma::make_map_3d(lv.x, es, lv.L.nx, lv.L.ny, lv.L.nz, lv.L.nx, 1);
+      lv.tm_em = tma::make_map_3d(cv.x, es, cv.L.nx, cv.L.ny, cv.L.nz, cv.L.nx, ty / 2);
+      lv.tm_eh = tma::make_map_3d(cv.x, es, cv.L.nx, cv.L.ny, cv.L.nz, cv.L.nx, 1);
+      lv.tma_prolong = true;
+    }
+    if(l == 0) {
+      const void* pp = P->precision == 1 ? static_cast<const void*>(P->p32) : P->p;
+      const int pes = P->precision == 1 ? 4 : 8;
+      P->tm_pm = tma::make_map_3d(pp, pes, lv.L.nx, lv.L.ny, lv.L.nz, lv.L.nx, ty);
+      P->tm_ph = tma::make_map_3d(pp, pes, lv.L.nx, lv.L.ny, lv.L.nz, lv.L.nx, 1);
+      P->tma_ap = true;
+    }
+  }
+  auto attr = [](const void* fn, size_t bytes) {
+    OFB_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)));
+  };
+  attr(reinterpret_cast<const void*>(k_tprolong<double, double, 4, 4>), tprolong_bytes<double, double>(256) * 4);
+  attr(reinterpret_cast<const void*>(k_tprolong<float, float, 4, 4>), tprolong_bytes<float, float>(256) * 4);
+  attr(reinterpret_cast<const void*>(k_tap<double, 4>), tround(static_cast<size_t>(6) * 256 * 8) * kTSlots);
+  attr(reinterpret_cast<const void*>(k_tap<float, 4>), tround(static_cast<size_t>(6) * 256 * 4) * kTSlots);
+  // the largest slot is that of nx = 256 (TY = 4): (TY + 2 + TY) rows of 256
+  OFB_CHECK(cudaFuncSetAttribute(k_tsmooth<double, double, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(tslot_bytes<double, double>(256) * kTSlots)));
+  OFB_CHECK(cudaFuncSetAttribute(k_tsmooth<float, float, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(tslot_bytes<float, float>(256) * kTSlots)));
+  OFB_CHECK(cudaFuncSetAttribute(k_tsmooth_pre<double, double, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(tslot_bytes<double, double>(256) * kTSlots)));
+  OFB_CHECK(cudaFuncSetAttribute(k_tsmooth_pre<float, float, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(tslot_bytes<float, float>(256) * kTSlots)));
+  OFB_CHECK(cudaFuncSetAttribute(k_tsmooth<double, double, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(tslot_bytes<double, double>(256) * kTSlots)));
+  OFB_CHECK(cudaFuncSetAttribute(k_tsmooth<float, float, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(tslot_bytes<float, float>(256) * kTSlots)));
+}
+
 }  // namespace
 
 PoissonPlan* poisson_plan_create(const Grid& g, const PBC& pbc_in, int precision) {
@@ -1557,6 +2333,14 @@ PoissonPlan* poisson_plan_create(const Grid& g, const PBC& pbc_in, int precision
     OFB_CHECK(cudaMemset(P->sc_in, 0, sizeof(SolveScalars)));
     P->bytes += 4 * nf * sizeof(float);
   }
+  {
+    int dev = 0;
+    OFB_CHECK(cudaGetDevice(&dev));
+    OFB_CHECK(cudaDeviceGetAttribute(&P->sms, cudaDevAttrMultiProcessorCount, dev));
+  }
+  OFB_CHECK(cudaMalloc(&P->fault, sizeof(int)));
+  OFB_CHECK(cudaMemset(P->fault, 0, sizeof(int)));
+  setup_tma(P, tsz);
   const char* no_graph = std::getenv("ORCHARD_B200_NO_GRAPH");
   P->use_graph = !(no_graph != nullptr && no_graph[0] == '1');
   return P;
@@ -1586,6 +2370,7 @@ void poisson_plan_destroy(PoissonPlan* P) {
   cudaFree(P->p32);
   cudaFree(P->ap32);
   cudaFree(P->sc_in);
+  cudaFree(P->fault);
   delete P;
 }
 
@@ -1621,6 +2406,21 @@ void launch_restrict(const Level& lv, const Level& cv, const B* b, const double*
     case 1: launch_restrict_r<T, B, 1, 1, 2>(lv, cv, b, sb_ptr, x, sx_ptr, bc, lsc, zm, lc, rb, s); break;
     default: launch_restrict_r<T, B, 1, 1, 1>(lv, cv, b, sb_ptr, x, sx_ptr, bc, lsc, zm, lc, rb, s); break;
   }
+}
+
+// Grid of a persistent plane-pipelined launch on a level: at most two blocks
+// per SM, each with a range of at least four tile-planes that fits kTMaxSeg
+// segments.
+struct TGrid {
+  int grid, ty;
+};
+
+TGrid tgrid(const PoissonPlan* P, const CLay& L) {
+  const int ty = 1024 / L.nx;
+  const long long items = static_cast<long long>(L.ny / ty) * L.nz;
+  long long g = std::min<long long>(2LL * P->sms, std::max(1LL, items / 4));
+  while((items / g + 1) / L.nz + 2 > kTMaxSeg) ++g;
+  return TGrid{static_cast<int>(g), ty};
 }
 
 // v_cycle (linsolve/poisson_solver.cpp:597-633) from level l; the finest
@@ -1665,8 +2465,13 @@ void v_cycle(PoissonPlan* P, int l, const V* r0, SolveScalars* sc, RedBuf rb, cu
     const bool vpr = vec && vec_enabled("prolong");
     const bool vre = vec && vec_enabled("restrict");
     const vst::RowLaunch lr = vst::row_launch(lv.L.nx, lv.L.ny, lv.L.nz, vst::Width<T>::W, 16);
-    if(vsm && vec_enabled("pre")) {
-      ProfScope ps(fine ? kKSmoothFine : kKCoarseLevels, s);
+    if(lv.tma && vec_enabled("tma")) {
+      ProfScope ps(fine ? kKSmoothFirstFine : kKCoarseLevels, s);
+      const TGrid tg = tgrid(P, lv.L);
+      k_tsmooth_pre<T, B, 4><<<tg.grid, 256, tround(static_cast<size_t>(tg.ty + 2) * lv.L.nx * sizeof(B)) * kTSlots, s>>>(
+          lv.op, lv.tm_bm, lv.tm_bh, sb_ptr, x, ls, zm, rb, P->fault);
+    } else if(vsm && vec_enabled("pre")) {
+      ProfScope ps(fine ? kKSmoothFirstFine : kKCoarseLevels, s);
       k_vsmooth_pre<T, B><<<lr.grid, lr.block, 0, s>>>(lv.op, bptr, sb_ptr, x, ls, zm, lr.kchunk, rb);
     } else {
       {
@@ -1695,7 +2500,13 @@ void v_cycle(PoissonPlan* P, int l, const V* r0, SolveScalars* sc, RedBuf rb, cu
     }
     OFB_LAUNCH_CHECK("v_cycle descent");
     v_cycle<T, V>(P, l + 1, r0, sc, rb, s);
-    {
+    if(lv.tma_prolong && vec_enabled("tma")) {
+      ProfScope ps(fine ? kKProlongFine : kKCoarseLevels, s);
+      const TGrid tg = tgrid(P, lv.L);
+      k_tprolong<T, B, 4, 4><<<tg.grid, 256, tprolong_bytes<T, B>(lv.L.nx) * 4, s>>>(
+          lv.op, lv.tm_xm, lv.tm_xh, lv.tm_bm, lv.tm_em, lv.tm_eh, sb_ptr, &ls->sx, &lsc->sx, a, ls, zm,
+          rb, P->fault);
+    } else {
       ProfScope ps(fine ? kKProlongFine : kKCoarseLevels, s);
       if(vpr)
         k_vprolong_smooth<T, B><<<lr.grid, lr.block, 0, s>>>(
@@ -1706,7 +2517,13 @@ void v_cycle(PoissonPlan* P, int l, const V* r0, SolveScalars* sc, RedBuf rb, cu
             lv.op, cv.L, bptr, sb_ptr, x, &ls->sx, static_cast<const T*>(cv.x), &lsc->sx, a, ls,
             lv.rx == 2 ? 1 : 0, lv.ry == 2 ? 1 : 0, lv.rz == 2 ? 1 : 0, zm, ln.kchunk, rb);
     }
-    {
+    if(lv.tma && vec_enabled("tma")) {
+      ProfScope ps(fine ? kKSmoothFine : kKCoarseLevels, s);
+      const TGrid tg = tgrid(P, lv.L);
+      const size_t sm = tslot_bytes<T, B>(lv.L.nx) * kTSlots;
+      k_tsmooth<T, B, 4><<<tg.grid, 256, sm, s>>>(lv.op, lv.tm_am, lv.tm_ah, lv.tm_bm, sb_ptr, &ls->sa, x,
+                                                  ls, zm, rz_sc, rb, P->fault);
+    } else {
       ProfScope ps(fine ? kKSmoothFine : kKCoarseLevels, s);
       if(vsm)
         k_vsmooth<T, B><<<lr.grid, lr.block, 0, s>>>(lv.op, bptr, sb_ptr, a, &ls->sa, x, ls, zm,
@@ -1759,7 +2576,11 @@ void enqueue_body(PoissonPlan* P, const CGVec<V>& v, SolveScalars* sc, RedBuf rb
   }
   {
     ProfScope ps(kKApplyAp, s);
-    if(vfits<V>(l0.L) && vec_enabled() && vec_enabled("ap")) {
+    if(P->tma_ap && vec_enabled("tma")) {
+      const TGrid tg = tgrid(P, l0.L);
+      k_tap<V, 4><<<tg.grid, 256, tround(static_cast<size_t>(tg.ty + 2) * l0.L.nx * sizeof(V)) * kTSlots, s>>>(
+          l0.op, P->tm_pm, P->tm_ph, v.ap, sc, rb, P->fault);
+    } else if(vfits<V>(l0.L) && vec_enabled() && vec_enabled("ap")) {
       const vst::RowLaunch lr = vst::row_launch(l0.L.nx, l0.L.ny, l0.L.nz, vst::Width<V>::W, 16);
       k_vapply_ap<V><<<lr.grid, lr.block, 0, s>>>(l0.op, v.p, v.ap, sc, lr.kchunk, rb);
     }
@@ -1979,6 +2800,12 @@ void poisson_solve(PoissonPlan* P, int max_iterations, double tolerance, SolveSc
     solve_dc<float>(P, max_iterations, tolerance, sc_dev, sc_host, rb, s, history, history_cap);
   else
     solve_impl<double>(P, max_iterations, tolerance, sc_dev, sc_host, rb, s, history, history_cap);
+  int fault = 0;
+  OFB_CHECK(cudaMemcpyAsync(&fault, P->fault, sizeof(int), cudaMemcpyDeviceToHost, s));
+  OFB_CHECK(cudaStreamSynchronize(s));
+  if(fault != 0)
+    throw TimeoutError("a bounded wait for a TMA plane load gave up in the pressure solve (code " +
+                       std::to_string(fault) + ")");
 }
 
 void launch_compact_to_pressure(const Grid& g, const double* x, const SolveScalars* sc,
