@@ -912,17 +912,8 @@ __global__ void __launch_bounds__(1024 / CPT)
 #pragma unroll
       for(int t = 0; t < CPT; ++t) v[t] = A(zs) * (v[t] - sin);
     };
-    A below[CPT], cen[CPT], above[CPT];
-    own(sg.lbase, below);
-    own(sg.lbase + 1, cen);
-    __syncthreads();
-    for(int k = sg.kb; k < sg.ke; ++k) {
-      const int c = sg.lbase + 1 + (k - sg.kb);  // load of plane k
-      if(threadIdx.x == 0) {
-        tma::fence_proxy_async();
-        while(next < nload && next <= c - 1 + D) issue(next++);
-      }
-      own(c + 1, above);
+    // one output plane k from its staged slot and the z-queue (below, cen, above)
+    auto plane = [&](int k, int c, const A (&below)[CPT], const A (&cen)[CPT], const A (&above)[CPT]) {
       const T* pk = uslot(c % D);
       const B* bk = bslot(c % D);
       A dn[CPT], up[CPT];
@@ -963,11 +954,29 @@ __global__ void __launch_bounds__(1024 / CPT)
       } else {
         *reinterpret_cast<float2*>(out + o.L.idx(i0, j, k)) = make_float2(v[0], v[1]);
       }
+    };
+    A q0[CPT], q1[CPT], q2[CPT], q3[CPT];
+    own(sg.lbase, q0);
+    own(sg.lbase + 1, q1);
+    __syncthreads();
+    // two planes per step (one when a single plane is left)
+    for(int k = sg.kb; k < sg.ke;) {
+      const int c = sg.lbase + 1 + (k - sg.kb);  // load of plane k
+      const bool two = k + 1 < sg.ke;
+      if(threadIdx.x == 0) {
+        tma::fence_proxy_async();
+        while(next < nload && next <= c - 1 + D) issue(next++);
+      }
+      own(c + 1, q2);
+      if(two) own(c + 2, q3);
+      plane(k, c, q0, q1, q2);
+      if(two) plane(k + 1, c + 1, q1, q2, q3);
 #pragma unroll
       for(int t = 0; t < CPT; ++t) {
-        below[t] = cen[t];
-        cen[t] = above[t];
+        q0[t] = two ? q2[t] : q1[t];
+        q1[t] = two ? q3[t] : q2[t];
       }
+      k += two ? 2 : 1;
       __syncthreads();
     }
   }
@@ -1425,6 +1434,169 @@ __global__ void __launch_bounds__(1024 / CPT)
       sc->alpha = sc->rz / pap;
     }
   });
+}
+
+// Residual + 2x2x2 restriction on the plane pipeline (same contract as
+// k_vrestrict): each step forms the residual (b - sb) - A (x - sx) on the two
+// fine planes of one coarse plane; a thread sums its cells pairwise in x and
+// over the two planes, and the row pairs are combined through shared memory.
+// The schedule runs over coarse planes, so each segment streams fine planes
+// 2 kc_begin - 1 .. 2 kc_end.
+template <typename T, typename B, int D>
+__global__ void __launch_bounds__(256)
+    k_trestrict(OpInfo o, OpInfo oc, const __grid_constant__ CUtensorMap xm,
+                const __grid_constant__ CUtensorMap xh, const __grid_constant__ CUtensorMap bm,
+                const double* sb_ptr, const double* sin_ptr, T* __restrict__ bc, LevelScalars* lsc,
+                int zm, RedBuf rb, int* fault) {
+  using A = T;
+  constexpr int CPT = 4;
+  extern __shared__ __align__(128) unsigned char tsm[];
+  __shared__ uint64_t bars[D];
+  const int NX = o.L.nx, NY = o.L.ny, NZ = o.L.nz;
+  const int TY = 1024 / NX;
+  const int tpr = NX / CPT;
+  const int r = threadIdx.x / tpr;
+  const int i0 = (threadIdx.x % tpr) * CPT;
+  const size_t ubytes = tround(static_cast<size_t>(TY + 2) * NX * sizeof(T));
+  const size_t sbytes = tslot_bytes<T, B>(NX);
+  const uint32_t tx_bytes = static_cast<uint32_t>((TY + 2) * NX * sizeof(T) + TY * NX * sizeof(B));
+  auto uslot = [&](int s) { return reinterpret_cast<T*>(tsm + s * sbytes); };
+  auto bslot = [&](int s) { return reinterpret_cast<B*>(tsm + s * sbytes + ubytes); };
+  A* part = reinterpret_cast<A*>(tsm + D * sbytes);  // [TY][NX / 2] row partials
+  // segments over coarse planes; loads count fine planes
+  TSeg seg[kTMaxSeg];
+  int nseg = 0, nload = 0;
+  {
+    const int nzc = NZ / 2;
+    const long long total = static_cast<long long>(NY / TY) * nzc;
+    const long long f0 = total * blockIdx.x / gridDim.x;
+    const long long f1 = total * (blockIdx.x + 1) / gridDim.x;
+    for(long long f = f0; f < f1 && nseg < kTMaxSeg;) {
+      const int tile = static_cast<int>(f / nzc);
+      const int kb = static_cast<int>(f % nzc);
+      const int ke = static_cast<int>(min(static_cast<long long>(nzc), kb + (f1 - f)));
+      seg[nseg++] = TSeg{tile, kb, ke, nload};
+      nload += 2 * (ke - kb) + 2;
+      f += ke - kb;
+    }
+  }
+  auto fine_plane = [&](const TSeg& sg, int l) { return 2 * sg.kb - 1 + (l - sg.lbase); };
+  auto issue = [&](int l) {
+    int q = 0;
+    while(q + 1 < nseg && seg[q + 1].lbase <= l) ++q;
+    const int j0 = seg[q].tile * TY;
+    int jm, jp;
+    double sg;
+    nb_lo(j0, NY, o.periodic[1], o.dir_lo[1], jm, sg);
+    nb_hi(j0 + TY - 1, NY, o.periodic[1], o.dir_hi[1], jp, sg);
+    const int kz = vst::zrow(fine_plane(seg[q], l), NZ, o.periodic[2], o.dir_lo[2], o.dir_hi[2], sg);
+    const int sl = l % D;
+    tma::mbar_arrive_expect_tx(&bars[sl], tx_bytes);
+    tma::load_3d(uslot(sl) + NX, &xm, &bars[sl], 0, j0, kz);
+    tma::load_3d(uslot(sl), &xh, &bars[sl], 0, jm, kz);
+    tma::load_3d(uslot(sl) + (TY + 1) * NX, &xh, &bars[sl], 0, jp, kz);
+    tma::load_3d(bslot(sl), &bm, &bars[sl], 0, j0, kz);
+  };
+  if(threadIdx.x == 0) {
+    for(int sl = 0; sl < D; ++sl) tma::mbar_init(&bars[sl], 1);
+    tma::fence_barrier_init();
+  }
+  __syncthreads();
+  int next = 0;
+  if(threadIdx.x == 0)
+    while(next < nload && next < D) issue(next++);
+  const double sb = *sb_ptr;
+  const A sin = A(*sin_ptr);
+  const A ix = A(o.inv2[0]), iy = A(o.inv2[1]), iz = A(o.inv2[2]);
+  double acc[1] = {0.0};
+  int xl, xr;
+  double sxl, sxr;
+  nb_lo(i0, NX, o.periodic[0], o.dir_lo[0], xl, sxl);
+  nb_hi(i0 + CPT - 1, NX, o.periodic[0], o.dir_hi[0], xr, sxr);
+  for(int q = 0; q < nseg; ++q) {
+    const TSeg sg = seg[q];
+    const int j0 = sg.tile * TY;
+    const int j = j0 + r;
+    int jm, jp;
+    double sylo, syhi;
+    nb_lo(j0, NY, o.periodic[1], o.dir_lo[1], jm, sylo);
+    nb_hi(j0 + TY - 1, NY, o.periodic[1], o.dir_hi[1], jp, syhi);
+    auto own = [&](int l, A (&v)[CPT]) {
+      tma::mbar_wait(&bars[l % D], (l / D) & 1, fault, 1);
+      double zs;
+      vst::zrow(fine_plane(sg, l), NZ, o.periodic[2], o.dir_lo[2], o.dir_hi[2], zs);
+      tload4<A>(uslot(l % D) + (r + 1) * NX + i0, v);
+#pragma unroll
+      for(int t = 0; t < CPT; ++t) v[t] = A(zs) * (v[t] - sin);
+    };
+    // residual of the CPT cells at the plane staged in load c
+    auto residual = [&](int c, const A (&below)[CPT], const A (&cen)[CPT], const A (&above)[CPT],
+                        A (&res)[CPT]) {
+      const T* pk = uslot(c % D);
+      const B* bk = bslot(c % D);
+      A dn[CPT], up[CPT];
+      tload4<A>(pk + r * NX + i0, dn);
+      tload4<A>(pk + (r + 2) * NX + i0, up);
+      const A sd = r == 0 ? A(sylo) : A(1), su = r == TY - 1 ? A(syhi) : A(1);
+#pragma unroll
+      for(int t = 0; t < CPT; ++t) {
+        dn[t] = sd * (dn[t] - sin);
+        up[t] = su * (up[t] - sin);
+      }
+      const A left = A(sxl) * (pk[(r + 1) * NX + xl] - sin);
+      const A right = A(sxr) * (pk[(r + 1) * NX + xr] - sin);
+      double bq[CPT];
+      tload4<double>(bk + r * NX + i0, bq);
+#pragma unroll
+      for(int t = 0; t < CPT; ++t) {
+        const A l = t > 0 ? cen[t - 1] : left;
+        const A rr = t < CPT - 1 ? cen[t + 1] : right;
+        const A two_c = A(2) * cen[t];
+        const A ax = -(rr - two_c + l) * ix - (up[t] - two_c + dn[t]) * iy - (above[t] - two_c + below[t]) * iz;
+        res[t] = A(bq[t] - sb) - ax;
+      }
+    };
+    A q0[CPT], q1[CPT], q2[CPT], q3[CPT];
+    own(sg.lbase, q0);
+    own(sg.lbase + 1, q1);
+    __syncthreads();
+    for(int kc = sg.kb; kc < sg.ke; ++kc) {
+      const int c = sg.lbase + 1 + 2 * (kc - sg.kb);  // load of fine plane 2 kc
+      if(threadIdx.x == 0) {
+        tma::fence_proxy_async();
+        while(next < nload && next <= c - 1 + D) issue(next++);
+      }
+      own(c + 1, q2);
+      own(c + 2, q3);
+      A r0[CPT], r1[CPT];
+      residual(c, q0, q1, q2, r0);
+      residual(c + 1, q1, q2, q3, r1);
+      part[r * (NX / 2) + (i0 >> 1)] = (r0[0] + r0[1]) + (r1[0] + r1[1]);
+      part[r * (NX / 2) + (i0 >> 1) + 1] = (r0[2] + r0[3]) + (r1[2] + r1[3]);
+#pragma unroll
+      for(int t = 0; t < CPT; ++t) {
+        q0[t] = q2[t];
+        q1[t] = q3[t];
+      }
+      __syncthreads();
+      if((r & 1) == 0) {
+        const int m = i0 >> 1;
+        const A c0 = A(0.125) * (part[r * (NX / 2) + m] + part[(r + 1) * (NX / 2) + m]);
+        const A c1 = A(0.125) * (part[r * (NX / 2) + m + 1] + part[(r + 1) * (NX / 2) + m + 1]);
+        T* dst = bc + oc.L.idx(m, j >> 1, kc);
+        if constexpr(std::is_same_v<T, double>) {
+          *reinterpret_cast<double2*>(dst) = make_double2(c0, c1);
+        } else {
+          *reinterpret_cast<float2*>(dst) = make_float2(c0, c1);
+        }
+        acc[0] += double(c0) + double(c1);
+      }
+      __syncthreads();
+    }
+  }
+  const bool mx[1] = {false};
+  const int n = oc.L.count();
+  reduce_finish<1>(acc, mx, rb, [=](const Sums<1>& st) { lsc->sb = zm ? st.v[0] / n : 0.0; });
 }
 
 // ---------------------------------------------------------------------------
@@ -2182,6 +2354,10 @@ void setup_tma(PoissonPlan* P, size_t tsz) {
   attr(reinterpret_cast<const void*>(k_tprolong<double, double, 4, 4>), tprolong_bytes<double, double>(256) * 4);
   attr(reinterpret_cast<const void*>(k_tprolong<float, float, 4, 4>), tprolong_bytes<float, float>(256) * 4);
   attr(reinterpret_cast<const void*>(k_tap<double, 4>), tround(static_cast<size_t>(6) * 256 * 8) * kTSlots);
+  attr(reinterpret_cast<const void*>(k_trestrict<double, double, kTSlots>),
+       tslot_bytes<double, double>(256) * kTSlots + 4 * 128 * 8);
+  attr(reinterpret_cast<const void*>(k_trestrict<float, float, kTSlots>),
+       tslot_bytes<float, float>(256) * kTSlots + 4 * 128 * 4);
   attr(reinterpret_cast<const void*>(k_tap<float, 4>), tround(static_cast<size_t>(6) * 256 * 4) * kTSlots);
   // the largest slot is that of nx = 256 (TY = 4): (TY + 2 + TY) rows of 256
   OFB_CHECK(cudaFuncSetAttribute(k_tsmooth<double, double, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -2486,7 +2662,17 @@ void v_cycle(PoissonPlan* P, int l, const V* r0, SolveScalars* sc, RedBuf rb, cu
         k_smooth<T, B><<<ln.grid, ln.block, 0, s>>>(lv.op, bptr, sb_ptr, a, &ls->sa, x, ls, 1, zm,
                                                     nullptr, ln.kchunk, rb);
     }
-    {
+    if(lv.tma_prolong && vec_enabled("tma")) {
+      ProfScope ps(fine ? kKRestrictFine : kKCoarseLevels, s);
+      const int ty = 1024 / lv.L.nx;
+      const long long items = static_cast<long long>(lv.L.ny / ty) * (lv.L.nz / 2);
+      long long g = std::min<long long>(2LL * P->sms, std::max(1LL, items / 2));
+      while((items / g + 1) / (lv.L.nz / 2) + 2 > kTMaxSeg) ++g;
+      const size_t sm = tslot_bytes<T, B>(lv.L.nx) * kTSlots + static_cast<size_t>(ty) * (lv.L.nx / 2) * sizeof(T);
+      k_trestrict<T, B, kTSlots><<<static_cast<int>(g), 256, sm, s>>>(
+          lv.op, cv.op, lv.tm_xm, lv.tm_xh, lv.tm_bm, sb_ptr, &ls->sx, static_cast<T*>(cv.b), lsc, zm, rb,
+          P->fault);
+    } else {
       ProfScope ps(fine ? kKRestrictFine : kKCoarseLevels, s);
       if(vre && lv.rx == 2 && lv.ry == 2 && lv.rz == 2) {
         const vst::RowLaunch lrc =
