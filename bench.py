@@ -62,25 +62,33 @@ def tg_dt(n, cfl=CFL):
 # ---------------------------------------------------------------------------
 
 def bytes_per_launch(n, precision):
+    """Compulsory bytes per launch of each kernel class.  FP64 path: every
+    pressure-solve vector is FP64.  Mixed path (defect correction): the inner
+    MG-PCG -- V-cycle and CG vectors alike -- is FP32 (s = 4); the outer FP64
+    kernels are the defect_correction class (three launches per correction:
+    rhs scaling 16 B, x update 20 B and residual 24 B per cell, 20 B average)."""
     N = n ** 3
     d = 8
-    t = 4 if precision == "mixed" else 8  # V-cycle level vectors
-    return {
+    s = 4 if precision == "mixed" else 8  # inner solve vectors
+    out = {
         "predictor_rhs": 5 * d * N,  # per component: read f, p, prev, adv; write rhs
         "advection": 4 * d * N,      # per component: read u, v, w; write adv
         "adi_sweep": 2 * d * N,
         "divergence_rhs": 5 * d * N,
         "pcg_initial_residual": 3 * d * N,
-        "pcg_apply_ap": 2 * d * N,
-        "pcg_update_xr": 6 * d * N,
-        "pcg_update_p": (2 * d + t) * N,
-        "vcycle_smooth_first_fine": (d + t) * N,
-        "vcycle_smooth_fine": (d + 2 * t) * N,
-        "vcycle_restrict_fine": (d + t + t / 8) * N,
-        "vcycle_prolong_smooth_fine": (d + 2 * t + t / 8) * N,
+        "pcg_apply_ap": 2 * s * N,
+        "pcg_update_xr": 6 * s * N,
+        "pcg_update_p": 3 * s * N,
+        "vcycle_smooth_first_fine": 2 * s * N,        # read b, write x
+        "vcycle_smooth_fine": 3 * s * N,              # read a, b; write x
+        "vcycle_restrict_fine": (2 + 1 / 8) * s * N,  # read b, x; write coarse b
+        "vcycle_prolong_smooth_fine": (3 + 1 / 8) * s * N,  # read x, b, coarse x; write a
         "correct_velocity": (1 + 3 + 3) * d * N / 3 + d * N,  # per component launch
         "cell_pass": 7 * d * N,
     }
+    if precision == "mixed":
+        out["defect_correction"] = 20 * N
+    return out
 
 
 def read_peaks():

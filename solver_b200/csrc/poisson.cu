@@ -2930,13 +2930,13 @@ void solve_dc(PoissonPlan* P, int max_iterations, double tolerance, SolveScalars
   const CGVec<float> v{nullptr, P->e32, P->r32, P->p32, P->ap32};
   SolveScalars* si = P->sc_in;
   auto pre = [&](cudaGraphConditionalHandle c) {
-    ProfScope ps(kKOther, s);
+    ProfScope ps(kKDefectCorrection, s);
     k_dc_to_inner<<<ln.grid, ln.block, 0, s>>>(l0.L, P->r, sc, P->r32, P->e32, si, ln.kchunk, rb, c);
     OFB_LAUNCH_CHECK("k_dc_to_inner");
   };
   auto body = [&](cudaGraphConditionalHandle c) { enqueue_body<T, float>(P, v, si, rb, s, c); };
   auto post = [&]() {
-    ProfScope ps(kKUpdateXr, s);
+    ProfScope ps(kKDefectCorrection, s, 2);
     k_dc_update_x<<<ln.grid, ln.block, 0, s>>>(l0.L, P->x, P->e32, sc, si, ln.kchunk, rb);
     k_dc_residual<<<ln.grid, ln.block, 0, s>>>(l0.op, P->b, P->x, P->r, sc, si, ln.kchunk, rb);
     OFB_LAUNCH_CHECK("defect correction update");

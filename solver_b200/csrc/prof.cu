@@ -52,7 +52,7 @@ const char* kNames[kKernelCount] = {
     "pcg_apply_ap", "pcg_update_xr", "pcg_update_p", "vcycle_smooth_first_fine",
     "vcycle_smooth_fine", "vcycle_restrict_fine", "vcycle_prolong_smooth_fine",
     "vcycle_coarse_levels", "vcycle_coarse_solve", "correct_velocity", "cell_pass",
-    "total_pressure_bc", "adjoint", "other"};
+    "total_pressure_bc", "adjoint", "defect_correction", "other"};
 
 }  // namespace
 

@@ -25,6 +25,7 @@ enum KernelClass : int {
   kKCellPass,
   kKTotalPressureBc,
   kKAdjoint,
+  kKDefectCorrection,
   kKOther,
   kKernelCount
 };
