@@ -821,7 +821,7 @@ __device__ __forceinline__ int tsegments(int tiles, int nz, TSeg (&seg)[kTMaxSeg
 // plane pipeline: out = x + omega (b - sb - A x) / D with x = in - s_in;
 // records mean(out) (ls->sx) and, on the finest level, r.z (sc).  Same
 // contract as k_vsmooth.  CPT cells per thread (4 or 2), 1024 / CPT threads.
-template <typename T, typename B, int CPT>
+template <typename T, typename B, int CPT, bool PER>
 __global__ void __launch_bounds__(1024 / CPT)
     k_tsmooth(OpInfo o, const __grid_constant__ CUtensorMap um, const __grid_constant__ CUtensorMap uh,
               const __grid_constant__ CUtensorMap bm, const double* sb_ptr, const double* sin_ptr,
@@ -909,8 +909,10 @@ __global__ void __launch_bounds__(1024 / CPT)
       double zs;
       vst::zrow(sg.kb - 1 + (l - sg.lbase), NZ, o.periodic[2], o.dir_lo[2], o.dir_hi[2], zs);
       ldrow(uslot(l % D) + (r + 1) * NX + i0, v);
+      if constexpr(!PER) {
 #pragma unroll
-      for(int t = 0; t < CPT; ++t) v[t] = A(zs) * (v[t] - sin);
+        for(int t = 0; t < CPT; ++t) v[t] = A(zs) * (v[t] - sin);
+      }
     };
     // one output plane k from its staged slot and the z-queue (below, cen, above)
     auto plane = [&](int k, int c, const A (&below)[CPT], const A (&cen)[CPT], const A (&above)[CPT]) {
@@ -919,14 +921,19 @@ __global__ void __launch_bounds__(1024 / CPT)
       A dn[CPT], up[CPT];
       ldrow(pk + r * NX + i0, dn);
       ldrow(pk + (r + 2) * NX + i0, up);
-      const A sd = r == 0 ? A(sylo) : A(1), su = r == TY - 1 ? A(syhi) : A(1);
+      A left = pk[(r + 1) * NX + xl], right = pk[(r + 1) * NX + xr];
+      if constexpr(!PER) {
+        // boundary signs and the mean shift (on a fully periodic grid the
+        // operator annihilates the shift, so raw values are used there)
+        const A sd = r == 0 ? A(sylo) : A(1), su = r == TY - 1 ? A(syhi) : A(1);
 #pragma unroll
-      for(int t = 0; t < CPT; ++t) {
-        dn[t] = sd * (dn[t] - sin);
-        up[t] = su * (up[t] - sin);
+        for(int t = 0; t < CPT; ++t) {
+          dn[t] = sd * (dn[t] - sin);
+          up[t] = su * (up[t] - sin);
+        }
+        left = A(sxl) * (left - sin);
+        right = A(sxr) * (right - sin);
       }
-      const A left = A(sxl) * (pk[(r + 1) * NX + xl] - sin);
-      const A right = A(sxr) * (pk[(r + 1) * NX + xr] - sin);
       double bq[CPT];
       if constexpr(CPT == 4) {
         tload4<double>(bk + r * NX + i0, bq);
@@ -943,7 +950,10 @@ __global__ void __launch_bounds__(1024 / CPT)
         const A rr = t < CPT - 1 ? cen[t + 1] : right;
         const A two_c = A(2) * cen[t];
         const A ax = -(rr - two_c + l) * ix - (up[t] - two_c + dn[t]) * iy - (above[t] - two_c + below[t]) * iz;
-        v[t] = cen[t] + om * (A(bd) - ax) * A(invd_s[cls[t] + cz]);
+        if constexpr(PER)
+          v[t] = (cen[t] - sin) + om * (A(bd) - ax) * A(invd_s[0]);
+        else
+          v[t] = cen[t] + om * (A(bd) - ax) * A(invd_s[cls[t] + cz]);
         acc[0] += double(v[t]);
         acc[1] += bd * double(v[t]);
       }
@@ -1002,7 +1012,7 @@ __global__ void __launch_bounds__(1024 / CPT)
 // (same contract as k_vsmooth_pre): the staged operand is b itself, and the
 // first sweep's a = omega (b - sb) / D is formed on read for every stencil
 // point, with the diagonal of the point's boundary image.
-template <typename T, typename B, int CPT>
+template <typename T, typename B, int CPT, bool PER>
 __global__ void __launch_bounds__(1024 / CPT)
     k_tsmooth_pre(OpInfo o, const __grid_constant__ CUtensorMap bm, const __grid_constant__ CUtensorMap bh,
                   const double* sb_ptr, T* __restrict__ out, LevelScalars* ls, int zm, RedBuf rb,
@@ -1093,8 +1103,14 @@ __global__ void __launch_bounds__(1024 / CPT)
       const int cz = 16 * axis_class(kz, NZ);
       double b[CPT];
       ldrow(slot(l % D) + (r + 1) * NX + i0, b);
+      if constexpr(PER) {
+        // raw b: the operator annihilates the constant omega sb / D
 #pragma unroll
-      for(int t = 0; t < CPT; ++t) v[t] = A(zs) * om * A(b[t] - sb) * A(invd_s[cown[t] + cz]);
+        for(int t = 0; t < CPT; ++t) v[t] = A(b[t]);
+      } else {
+#pragma unroll
+        for(int t = 0; t < CPT; ++t) v[t] = A(zs) * om * A(b[t] - sb) * A(invd_s[cown[t] + cz]);
+      }
     };
     A below[CPT], cen[CPT], above[CPT];
     own(sg.lbase, below);
@@ -1113,22 +1129,39 @@ __global__ void __launch_bounds__(1024 / CPT)
       ldrow(pk + r * NX + i0, bd);
       ldrow(pk + (r + 2) * NX + i0, bu);
       ldrow(pk + (r + 1) * NX + i0, bc);
-      A dn[CPT], up[CPT];
+      A dn[CPT], up[CPT], left, right;
+      if constexpr(PER) {
 #pragma unroll
-      for(int t = 0; t < CPT; ++t) {
-        dn[t] = sd * om * A(bd[t] - sb) * A(invd_s[cdn[t] + cz]);
-        up[t] = su * om * A(bu[t] - sb) * A(invd_s[cup[t] + cz]);
+        for(int t = 0; t < CPT; ++t) {
+          dn[t] = A(bd[t]);
+          up[t] = A(bu[t]);
+        }
+        left = A(pk[(r + 1) * NX + xl]);
+        right = A(pk[(r + 1) * NX + xr]);
+      } else {
+#pragma unroll
+        for(int t = 0; t < CPT; ++t) {
+          dn[t] = sd * om * A(bd[t] - sb) * A(invd_s[cdn[t] + cz]);
+          up[t] = su * om * A(bu[t] - sb) * A(invd_s[cup[t] + cz]);
+        }
+        left = A(sxl) * om * A(double(pk[(r + 1) * NX + xl]) - sb) * A(invd_s[cl + cz]);
+        right = A(sxr) * om * A(double(pk[(r + 1) * NX + xr]) - sb) * A(invd_s[cr + cz]);
       }
-      const A left = A(sxl) * om * A(double(pk[(r + 1) * NX + xl]) - sb) * A(invd_s[cl + cz]);
-      const A right = A(sxr) * om * A(double(pk[(r + 1) * NX + xr]) - sb) * A(invd_s[cr + cz]);
       A v[CPT];
+      const A w0 = om * A(invd_s[0]);
 #pragma unroll
       for(int t = 0; t < CPT; ++t) {
         const A l = t > 0 ? cen[t - 1] : left;
         const A rr = t < CPT - 1 ? cen[t + 1] : right;
         const A two_c = A(2) * cen[t];
         const A ax = -(rr - two_c + l) * ix - (up[t] - two_c + dn[t]) * iy - (above[t] - two_c + below[t]) * iz;
-        v[t] = cen[t] + om * (A(bc[t] - sb) - ax) * A(invd_s[cown[t] + cz]);
+        if constexpr(PER) {
+          // a = w (b - sb) on every point, so A a = w A b
+          const A bcs = A(bc[t] - sb);
+          v[t] = w0 * bcs + w0 * (bcs - w0 * ax);
+        } else {
+          v[t] = cen[t] + om * (A(bc[t] - sb) - ax) * A(invd_s[cown[t] + cz]);
+        }
         acc[0] += double(v[t]);
       }
       if constexpr(CPT == 4) {
@@ -1158,7 +1191,7 @@ __global__ void __launch_bounds__(1024 / CPT)
 // contract as k_vprolong_smooth, 2x2x2 coarsening): the staged operand is the
 // level's correction x and the coarse correction ec (parent rows and the
 // parents of the halo rows), combined on read as (x - sx) + (ec - sec).
-template <typename T, typename B, int CPT, int D>
+template <typename T, typename B, int CPT, int D, bool PER>
 __global__ void __launch_bounds__(1024 / CPT)
     k_tprolong(OpInfo o, const __grid_constant__ CUtensorMap xm, const __grid_constant__ CUtensorMap xh,
                const __grid_constant__ CUtensorMap bm, const __grid_constant__ CUtensorMap em,
@@ -1226,15 +1259,18 @@ __global__ void __launch_bounds__(1024 / CPT)
   // fine slot row (0 .. TY+1) -> coarse slot row of its parent
   auto crow = [&](int fr) { return fr == 0 ? 0 : (fr == TY + 1 ? TYc + 1 : ((fr - 1) >> 1) + 1); };
   // combined operand of the CPT cells at fine slot row fr (shifted, unsigned)
+  // (on a fully periodic grid the shifts are left out: the operator
+  // annihilates constants, and only the centre value needs them)
+  const A shx = PER ? A(0) : sin, she = PER ? A(0) : sec;
   auto operand = [&](const T* xs, const T* es, int fr, A (&v)[CPT]) {
     A xv[CPT];
     tload4<A>(xs + fr * NX + i0, xv);
     const T* erow = es + crow(fr) * NXc + (i0 >> 1);
-    const A e0 = A(erow[0]) - sec, e1 = A(erow[1]) - sec;
-    v[0] = (xv[0] - sin) + e0;
-    v[1] = (xv[1] - sin) + e0;
-    v[2] = (xv[2] - sin) + e1;
-    v[3] = (xv[3] - sin) + e1;
+    const A e0 = A(erow[0]) - she, e1 = A(erow[1]) - she;
+    v[0] = (xv[0] - shx) + e0;
+    v[1] = (xv[1] - shx) + e0;
+    v[2] = (xv[2] - shx) + e1;
+    v[3] = (xv[3] - shx) + e1;
   };
   double acc[1] = {0.0};
   int xl, xr;
@@ -1257,8 +1293,10 @@ __global__ void __launch_bounds__(1024 / CPT)
       double zs;
       vst::zrow(sg.kb - 1 + (l - sg.lbase), NZ, o.periodic[2], o.dir_lo[2], o.dir_hi[2], zs);
       operand(xslot(l % D), eslot(l % D), r + 1, v);
+      if constexpr(!PER) {
 #pragma unroll
-      for(int t = 0; t < CPT; ++t) v[t] *= A(zs);
+        for(int t = 0; t < CPT; ++t) v[t] *= A(zs);
+      }
     };
     A below[CPT], cen[CPT], above[CPT];
     own(sg.lbase, below);
@@ -1277,15 +1315,21 @@ __global__ void __launch_bounds__(1024 / CPT)
       A dn[CPT], up[CPT];
       operand(xs, es, r, dn);
       operand(xs, es, r + 2, up);
-      const A sd = r == 0 ? A(sylo) : A(1), su = r == TY - 1 ? A(syhi) : A(1);
+      if constexpr(!PER) {
+        const A sd = r == 0 ? A(sylo) : A(1), su = r == TY - 1 ? A(syhi) : A(1);
 #pragma unroll
-      for(int t = 0; t < CPT; ++t) {
-        dn[t] *= sd;
-        up[t] *= su;
+        for(int t = 0; t < CPT; ++t) {
+          dn[t] *= sd;
+          up[t] *= su;
+        }
       }
       const T* erow = es + crow(r + 1) * NXc;
-      const A left = A(sxl) * ((A(xs[(r + 1) * NX + xl]) - sin) + (A(erow[xl >> 1]) - sec));
-      const A right = A(sxr) * ((A(xs[(r + 1) * NX + xr]) - sin) + (A(erow[xr >> 1]) - sec));
+      A left = (A(xs[(r + 1) * NX + xl]) - shx) + (A(erow[xl >> 1]) - she);
+      A right = (A(xs[(r + 1) * NX + xr]) - shx) + (A(erow[xr >> 1]) - she);
+      if constexpr(!PER) {
+        left *= A(sxl);
+        right *= A(sxr);
+      }
       double bq[CPT];
       tload4<double>(bk + r * NX + i0, bq);
       const int cz = 16 * axis_class(k, NZ);
@@ -1296,7 +1340,10 @@ __global__ void __launch_bounds__(1024 / CPT)
         const A rr = t < CPT - 1 ? cen[t + 1] : right;
         const A two_c = A(2) * cen[t];
         const A ax = -(rr - two_c + l) * ix - (up[t] - two_c + dn[t]) * iy - (above[t] - two_c + below[t]) * iz;
-        v[t] = cen[t] + om * (A(bq[t] - sb) - ax) * A(invd_s[cls[t] + cz]);
+        if constexpr(PER)
+          v[t] = (cen[t] - sin - sec) + om * (A(bq[t] - sb) - ax) * A(invd_s[0]);
+        else
+          v[t] = cen[t] + om * (A(bq[t] - sb) - ax) * A(invd_s[cls[t] + cz]);
         acc[0] += double(v[t]);
       }
       tstore4<T>(out + o.L.idx(i0, j, k), v);
@@ -1314,7 +1361,7 @@ __global__ void __launch_bounds__(1024 / CPT)
 }
 
 // A p on the plane pipeline (same contract as k_vapply_ap).
-template <typename V, int CPT>
+template <typename V, int CPT, bool PER>
 __global__ void __launch_bounds__(1024 / CPT)
     k_tap(OpInfo o, const __grid_constant__ CUtensorMap pm, const __grid_constant__ CUtensorMap ph,
           V* __restrict__ ap, SolveScalars* sc, RedBuf rb, int* fault) {
@@ -1376,8 +1423,10 @@ __global__ void __launch_bounds__(1024 / CPT)
       double zs;
       vst::zrow(sg.kb - 1 + (l - sg.lbase), NZ, o.periodic[2], o.dir_lo[2], o.dir_hi[2], zs);
       tload4<double>(slot(l % D) + (r + 1) * NX + i0, v);
+      if constexpr(!PER) {
 #pragma unroll
-      for(int t = 0; t < CPT; ++t) v[t] = zs * (v[t] - sp);
+        for(int t = 0; t < CPT; ++t) v[t] = zs * (v[t] - sp);
+      }
     };
     double below[CPT], cen[CPT], above[CPT];
     own(sg.lbase, below);
@@ -1394,14 +1443,17 @@ __global__ void __launch_bounds__(1024 / CPT)
       double dn[CPT], up[CPT];
       tload4<double>(pk + r * NX + i0, dn);
       tload4<double>(pk + (r + 2) * NX + i0, up);
-      const double sd = r == 0 ? sylo : 1.0, su = r == TY - 1 ? syhi : 1.0;
+      double left = double(pk[(r + 1) * NX + xl]), right = double(pk[(r + 1) * NX + xr]);
+      if constexpr(!PER) {
+        const double sd = r == 0 ? sylo : 1.0, su = r == TY - 1 ? syhi : 1.0;
 #pragma unroll
-      for(int t = 0; t < CPT; ++t) {
-        dn[t] = sd * (dn[t] - sp);
-        up[t] = su * (up[t] - sp);
+        for(int t = 0; t < CPT; ++t) {
+          dn[t] = sd * (dn[t] - sp);
+          up[t] = su * (up[t] - sp);
+        }
+        left = sxl * (left - sp);
+        right = sxr * (right - sp);
       }
-      const double left = sxl * (double(pk[(r + 1) * NX + xl]) - sp);
-      const double right = sxr * (double(pk[(r + 1) * NX + xr]) - sp);
       double v[CPT];
 #pragma unroll
       for(int t = 0; t < CPT; ++t) {
@@ -1409,9 +1461,10 @@ __global__ void __launch_bounds__(1024 / CPT)
         const double rr = t < CPT - 1 ? cen[t + 1] : right;
         const double two_c = 2.0 * cen[t];
         v[t] = -(rr - two_c + l) * ix - (up[t] - two_c + dn[t]) * iy - (above[t] - two_c + below[t]) * iz;
+        const double cs = PER ? cen[t] - sp : cen[t];
         acc[0] += v[t];
-        acc[1] += cen[t] * v[t];
-        acc[2] += cen[t];
+        acc[1] += cs * v[t];
+        acc[2] += cs;
       }
       tstore4<V>(ap + o.L.idx(i0, j, k), v);
 #pragma unroll
@@ -1442,7 +1495,7 @@ __global__ void __launch_bounds__(1024 / CPT)
 // over the two planes, and the row pairs are combined through shared memory.
 // The schedule runs over coarse planes, so each segment streams fine planes
 // 2 kc_begin - 1 .. 2 kc_end.
-template <typename T, typename B, int D>
+template <typename T, typename B, int D, bool PER>
 __global__ void __launch_bounds__(256)
     k_trestrict(OpInfo o, OpInfo oc, const __grid_constant__ CUtensorMap xm,
                 const __grid_constant__ CUtensorMap xh, const __grid_constant__ CUtensorMap bm,
@@ -1526,8 +1579,10 @@ __global__ void __launch_bounds__(256)
       double zs;
       vst::zrow(fine_plane(sg, l), NZ, o.periodic[2], o.dir_lo[2], o.dir_hi[2], zs);
       tload4<A>(uslot(l % D) + (r + 1) * NX + i0, v);
+      if constexpr(!PER) {
 #pragma unroll
-      for(int t = 0; t < CPT; ++t) v[t] = A(zs) * (v[t] - sin);
+        for(int t = 0; t < CPT; ++t) v[t] = A(zs) * (v[t] - sin);
+      }
     };
     // residual of the CPT cells at the plane staged in load c
     auto residual = [&](int c, const A (&below)[CPT], const A (&cen)[CPT], const A (&above)[CPT],
@@ -1537,14 +1592,17 @@ __global__ void __launch_bounds__(256)
       A dn[CPT], up[CPT];
       tload4<A>(pk + r * NX + i0, dn);
       tload4<A>(pk + (r + 2) * NX + i0, up);
-      const A sd = r == 0 ? A(sylo) : A(1), su = r == TY - 1 ? A(syhi) : A(1);
+      A left = pk[(r + 1) * NX + xl], right = pk[(r + 1) * NX + xr];
+      if constexpr(!PER) {
+        const A sd = r == 0 ? A(sylo) : A(1), su = r == TY - 1 ? A(syhi) : A(1);
 #pragma unroll
-      for(int t = 0; t < CPT; ++t) {
-        dn[t] = sd * (dn[t] - sin);
-        up[t] = su * (up[t] - sin);
+        for(int t = 0; t < CPT; ++t) {
+          dn[t] = sd * (dn[t] - sin);
+          up[t] = su * (up[t] - sin);
+        }
+        left = A(sxl) * (left - sin);
+        right = A(sxr) * (right - sin);
       }
-      const A left = A(sxl) * (pk[(r + 1) * NX + xl] - sin);
-      const A right = A(sxr) * (pk[(r + 1) * NX + xr] - sin);
       double bq[CPT];
       tload4<double>(bk + r * NX + i0, bq);
 #pragma unroll
@@ -2163,6 +2221,7 @@ struct PoissonPlan {
   int* fault = nullptr;  // device: a bounded wait in a plane-pipelined kernel gave up
   int sms = 148;         // streaming multiprocessors of the plan's device
   bool tma_ap = false;   // plane-pipelined A p on the finest level
+  bool all_periodic = false;  // every face periodic: constant diagonal, no boundary signs
   CUtensorMap tm_pm, tm_ph;
   // levels tail_first.. run as one single-block launch (k_vcycle_tail)
   int tail_first = -1;
@@ -2351,27 +2410,36 @@ void setup_tma(PoissonPlan* P, size_t tsz) {
   auto attr = [](const void* fn, size_t bytes) {
     OFB_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)));
   };
-  attr(reinterpret_cast<const void*>(k_tprolong<double, double, 4, 4>), tprolong_bytes<double, double>(256) * 4);
-  attr(reinterpret_cast<const void*>(k_tprolong<float, float, 4, 4>), tprolong_bytes<float, float>(256) * 4);
-  attr(reinterpret_cast<const void*>(k_tap<double, 4>), tround(static_cast<size_t>(6) * 256 * 8) * kTSlots);
-  attr(reinterpret_cast<const void*>(k_trestrict<double, double, kTSlots>),
+  attr(reinterpret_cast<const void*>(k_tprolong<double, double, 4, 4, false>), tprolong_bytes<double, double>(256) * 4);
+  attr(reinterpret_cast<const void*>(k_tprolong<double, double, 4, 4, true>), tprolong_bytes<double, double>(256) * 4);
+  attr(reinterpret_cast<const void*>(k_tprolong<float, float, 4, 4, false>), tprolong_bytes<float, float>(256) * 4);
+  attr(reinterpret_cast<const void*>(k_tprolong<float, float, 4, 4, true>), tprolong_bytes<float, float>(256) * 4);
+  attr(reinterpret_cast<const void*>(k_tap<double, 4, false>), tround(static_cast<size_t>(6) * 256 * 8) * kTSlots);
+  attr(reinterpret_cast<const void*>(k_tap<double, 4, true>), tround(static_cast<size_t>(6) * 256 * 8) * kTSlots);
+  attr(reinterpret_cast<const void*>(k_tap<float, 4, false>), tround(static_cast<size_t>(6) * 256 * 4) * kTSlots);
+  attr(reinterpret_cast<const void*>(k_tap<float, 4, true>), tround(static_cast<size_t>(6) * 256 * 4) * kTSlots);
+  attr(reinterpret_cast<const void*>(k_trestrict<double, double, kTSlots, false>),
        tslot_bytes<double, double>(256) * kTSlots + 4 * 128 * 8);
-  attr(reinterpret_cast<const void*>(k_trestrict<float, float, kTSlots>),
+  attr(reinterpret_cast<const void*>(k_trestrict<double, double, kTSlots, true>),
+       tslot_bytes<double, double>(256) * kTSlots + 4 * 128 * 8);
+  attr(reinterpret_cast<const void*>(k_trestrict<float, float, kTSlots, false>),
        tslot_bytes<float, float>(256) * kTSlots + 4 * 128 * 4);
-  attr(reinterpret_cast<const void*>(k_tap<float, 4>), tround(static_cast<size_t>(6) * 256 * 4) * kTSlots);
+  attr(reinterpret_cast<const void*>(k_trestrict<float, float, kTSlots, true>),
+       tslot_bytes<float, float>(256) * kTSlots + 4 * 128 * 4);
   // the largest slot is that of nx = 256 (TY = 4): (TY + 2 + TY) rows of 256
-  OFB_CHECK(cudaFuncSetAttribute(k_tsmooth<double, double, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(tslot_bytes<double, double>(256) * kTSlots)));
-  OFB_CHECK(cudaFuncSetAttribute(k_tsmooth<float, float, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(tslot_bytes<float, float>(256) * kTSlots)));
-  OFB_CHECK(cudaFuncSetAttribute(k_tsmooth_pre<double, double, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(tslot_bytes<double, double>(256) * kTSlots)));
-  OFB_CHECK(cudaFuncSetAttribute(k_tsmooth_pre<float, float, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(tslot_bytes<float, float>(256) * kTSlots)));
-  OFB_CHECK(cudaFuncSetAttribute(k_tsmooth<double, double, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(tslot_bytes<double, double>(256) * kTSlots)));
-  OFB_CHECK(cudaFuncSetAttribute(k_tsmooth<float, float, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(tslot_bytes<float, float>(256) * kTSlots)));
+  for(const void* fn : {reinterpret_cast<const void*>(k_tsmooth<double, double, 4, false>),
+                         reinterpret_cast<const void*>(k_tsmooth<double, double, 4, true>)})
+    attr(fn, tslot_bytes<double, double>(256) * kTSlots);
+  for(const void* fn : {reinterpret_cast<const void*>(k_tsmooth<float, float, 4, false>),
+                         reinterpret_cast<const void*>(k_tsmooth<float, float, 4, true>)})
+    attr(fn, tslot_bytes<float, float>(256) * kTSlots);
+  for(const void* fn : {reinterpret_cast<const void*>(k_tsmooth_pre<double, double, 4, false>),
+                         reinterpret_cast<const void*>(k_tsmooth_pre<double, double, 4, true>)})
+    attr(fn, tslot_bytes<double, double>(256) * kTSlots);
+  for(const void* fn : {reinterpret_cast<const void*>(k_tsmooth_pre<float, float, 4, false>),
+                         reinterpret_cast<const void*>(k_tsmooth_pre<float, float, 4, true>)})
+    attr(fn, tslot_bytes<float, float>(256) * kTSlots);
+
 }
 
 }  // namespace
@@ -2516,6 +2584,9 @@ PoissonPlan* poisson_plan_create(const Grid& g, const PBC& pbc_in, int precision
   }
   OFB_CHECK(cudaMalloc(&P->fault, sizeof(int)));
   OFB_CHECK(cudaMemset(P->fault, 0, sizeof(int)));
+  P->all_periodic = true;
+  for(int f = 0; f < 6; ++f)
+    if(P->pbc.type[f] != kPPeriodic) P->all_periodic = false;
   setup_tma(P, tsz);
   const char* no_graph = std::getenv("ORCHARD_B200_NO_GRAPH");
   P->use_graph = !(no_graph != nullptr && no_graph[0] == '1');
@@ -2644,8 +2715,13 @@ void v_cycle(PoissonPlan* P, int l, const V* r0, SolveScalars* sc, RedBuf rb, cu
     if(lv.tma && vec_enabled("tma")) {
       ProfScope ps(fine ? kKSmoothFirstFine : kKCoarseLevels, s);
       const TGrid tg = tgrid(P, lv.L);
-      k_tsmooth_pre<T, B, 4><<<tg.grid, 256, tround(static_cast<size_t>(tg.ty + 2) * lv.L.nx * sizeof(B)) * kTSlots, s>>>(
-          lv.op, lv.tm_bm, lv.tm_bh, sb_ptr, x, ls, zm, rb, P->fault);
+      const size_t sm = tround(static_cast<size_t>(tg.ty + 2) * lv.L.nx * sizeof(B)) * kTSlots;
+      if(P->all_periodic)
+        k_tsmooth_pre<T, B, 4, true><<<tg.grid, 256, sm, s>>>(lv.op, lv.tm_bm, lv.tm_bh, sb_ptr, x, ls, zm, rb,
+                                                              P->fault);
+      else
+        k_tsmooth_pre<T, B, 4, false><<<tg.grid, 256, sm, s>>>(lv.op, lv.tm_bm, lv.tm_bh, sb_ptr, x, ls, zm,
+                                                               rb, P->fault);
     } else if(vsm && vec_enabled("pre")) {
       ProfScope ps(fine ? kKSmoothFirstFine : kKCoarseLevels, s);
       k_vsmooth_pre<T, B><<<lr.grid, lr.block, 0, s>>>(lv.op, bptr, sb_ptr, x, ls, zm, lr.kchunk, rb);
@@ -2669,9 +2745,14 @@ void v_cycle(PoissonPlan* P, int l, const V* r0, SolveScalars* sc, RedBuf rb, cu
       long long g = std::min<long long>(2LL * P->sms, std::max(1LL, items / 2));
       while((items / g + 1) / (lv.L.nz / 2) + 2 > kTMaxSeg) ++g;
       const size_t sm = tslot_bytes<T, B>(lv.L.nx) * kTSlots + static_cast<size_t>(ty) * (lv.L.nx / 2) * sizeof(T);
-      k_trestrict<T, B, kTSlots><<<static_cast<int>(g), 256, sm, s>>>(
-          lv.op, cv.op, lv.tm_xm, lv.tm_xh, lv.tm_bm, sb_ptr, &ls->sx, static_cast<T*>(cv.b), lsc, zm, rb,
-          P->fault);
+      if(P->all_periodic)
+        k_trestrict<T, B, kTSlots, true><<<static_cast<int>(g), 256, sm, s>>>(
+            lv.op, cv.op, lv.tm_xm, lv.tm_xh, lv.tm_bm, sb_ptr, &ls->sx, static_cast<T*>(cv.b), lsc, zm, rb,
+            P->fault);
+      else
+        k_trestrict<T, B, kTSlots, false><<<static_cast<int>(g), 256, sm, s>>>(
+            lv.op, cv.op, lv.tm_xm, lv.tm_xh, lv.tm_bm, sb_ptr, &ls->sx, static_cast<T*>(cv.b), lsc, zm, rb,
+            P->fault);
     } else {
       ProfScope ps(fine ? kKRestrictFine : kKCoarseLevels, s);
       if(vre && lv.rx == 2 && lv.ry == 2 && lv.rz == 2) {
@@ -2689,9 +2770,14 @@ void v_cycle(PoissonPlan* P, int l, const V* r0, SolveScalars* sc, RedBuf rb, cu
     if(lv.tma_prolong && vec_enabled("tma")) {
       ProfScope ps(fine ? kKProlongFine : kKCoarseLevels, s);
       const TGrid tg = tgrid(P, lv.L);
-      k_tprolong<T, B, 4, 4><<<tg.grid, 256, tprolong_bytes<T, B>(lv.L.nx) * 4, s>>>(
-          lv.op, lv.tm_xm, lv.tm_xh, lv.tm_bm, lv.tm_em, lv.tm_eh, sb_ptr, &ls->sx, &lsc->sx, a, ls, zm,
-          rb, P->fault);
+      if(P->all_periodic)
+        k_tprolong<T, B, 4, 4, true><<<tg.grid, 256, tprolong_bytes<T, B>(lv.L.nx) * 4, s>>>(
+            lv.op, lv.tm_xm, lv.tm_xh, lv.tm_bm, lv.tm_em, lv.tm_eh, sb_ptr, &ls->sx, &lsc->sx, a, ls, zm,
+            rb, P->fault);
+      else
+        k_tprolong<T, B, 4, 4, false><<<tg.grid, 256, tprolong_bytes<T, B>(lv.L.nx) * 4, s>>>(
+            lv.op, lv.tm_xm, lv.tm_xh, lv.tm_bm, lv.tm_em, lv.tm_eh, sb_ptr, &ls->sx, &lsc->sx, a, ls, zm,
+            rb, P->fault);
     } else {
       ProfScope ps(fine ? kKProlongFine : kKCoarseLevels, s);
       if(vpr)
@@ -2707,8 +2793,12 @@ void v_cycle(PoissonPlan* P, int l, const V* r0, SolveScalars* sc, RedBuf rb, cu
       ProfScope ps(fine ? kKSmoothFine : kKCoarseLevels, s);
       const TGrid tg = tgrid(P, lv.L);
       const size_t sm = tslot_bytes<T, B>(lv.L.nx) * kTSlots;
-      k_tsmooth<T, B, 4><<<tg.grid, 256, sm, s>>>(lv.op, lv.tm_am, lv.tm_ah, lv.tm_bm, sb_ptr, &ls->sa, x,
-                                                  ls, zm, rz_sc, rb, P->fault);
+      if(P->all_periodic)
+        k_tsmooth<T, B, 4, true><<<tg.grid, 256, sm, s>>>(lv.op, lv.tm_am, lv.tm_ah, lv.tm_bm, sb_ptr, &ls->sa,
+                                                          x, ls, zm, rz_sc, rb, P->fault);
+      else
+        k_tsmooth<T, B, 4, false><<<tg.grid, 256, sm, s>>>(lv.op, lv.tm_am, lv.tm_ah, lv.tm_bm, sb_ptr,
+                                                           &ls->sa, x, ls, zm, rz_sc, rb, P->fault);
     } else {
       ProfScope ps(fine ? kKSmoothFine : kKCoarseLevels, s);
       if(vsm)
@@ -2764,8 +2854,11 @@ void enqueue_body(PoissonPlan* P, const CGVec<V>& v, SolveScalars* sc, RedBuf rb
     ProfScope ps(kKApplyAp, s);
     if(P->tma_ap && vec_enabled("tma")) {
       const TGrid tg = tgrid(P, l0.L);
-      k_tap<V, 4><<<tg.grid, 256, tround(static_cast<size_t>(tg.ty + 2) * l0.L.nx * sizeof(V)) * kTSlots, s>>>(
-          l0.op, P->tm_pm, P->tm_ph, v.ap, sc, rb, P->fault);
+      const size_t sm = tround(static_cast<size_t>(tg.ty + 2) * l0.L.nx * sizeof(V)) * kTSlots;
+      if(P->all_periodic)
+        k_tap<V, 4, true><<<tg.grid, 256, sm, s>>>(l0.op, P->tm_pm, P->tm_ph, v.ap, sc, rb, P->fault);
+      else
+        k_tap<V, 4, false><<<tg.grid, 256, sm, s>>>(l0.op, P->tm_pm, P->tm_ph, v.ap, sc, rb, P->fault);
     } else if(vfits<V>(l0.L) && vec_enabled() && vec_enabled("ap")) {
       const vst::RowLaunch lr = vst::row_launch(l0.L.nx, l0.L.ny, l0.L.nz, vst::Width<V>::W, 16);
       k_vapply_ap<V><<<lr.grid, lr.block, 0, s>>>(l0.op, v.p, v.ap, sc, lr.kchunk, rb);
