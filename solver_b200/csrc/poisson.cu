@@ -1489,6 +1489,267 @@ __global__ void __launch_bounds__(1024 / CPT)
   });
 }
 
+// Fused CG step on the plane pipeline: p = (z - sz) + beta (p_old - sp_old)
+// (p = z - sz on the first body), A p, and the previous iteration's deferred
+// solution update x = (x - sx) + alpha_old (p_old - sp_old)
+// (linsolve/poisson_solver.cpp:762-766, one body later).  The staged operand
+// is z + beta p_old: the operator annihilates the mean shifts wherever they
+// are nonzero (periodic / all-Neumann problems).  Records sp, sap, pap and
+// alpha as k_update_p and k_apply_ap do, and mean(x).
+template <typename T, typename V, bool PER>
+__global__ void __launch_bounds__(256)
+    k_tpap(OpInfo o, const __grid_constant__ CUtensorMap zm_, const __grid_constant__ CUtensorMap zh,
+           const __grid_constant__ CUtensorMap pm0, const __grid_constant__ CUtensorMap ph0,
+           const __grid_constant__ CUtensorMap pm1, const __grid_constant__ CUtensorMap ph1,
+           const LevelScalars* ls0, V* p0, V* p1, V* __restrict__ ap, V* __restrict__ x,
+           SolveScalars* sc, RedBuf rb, int* fault) {
+  constexpr int CPT = 4;
+  constexpr int D = 4;
+  extern __shared__ __align__(128) unsigned char tsm[];
+  __shared__ uint64_t bars[D];
+  const int NX = o.L.nx, NY = o.L.ny, NZ = o.L.nz;
+  const int TY = 1024 / NX;
+  const int tpr = NX / CPT;
+  const int r = threadIdx.x / tpr;
+  const int i0 = (threadIdx.x % tpr) * CPT;
+  const size_t zbytes = tround(static_cast<size_t>(TY + 2) * NX * sizeof(T));
+  const size_t sbytes = zbytes + tround(static_cast<size_t>(TY + 2) * NX * sizeof(V));
+  const uint32_t tx_bytes = static_cast<uint32_t>((TY + 2) * NX * (sizeof(T) + sizeof(V)));
+  auto zslot = [&](int s) { return reinterpret_cast<T*>(tsm + s * sbytes); };
+  auto pslot = [&](int s) { return reinterpret_cast<V*>(tsm + s * sbytes + zbytes); };
+  // p ping-pongs between two buffers: body b reads p_old from buffer
+  // (b + 1) & 1 and writes p to buffer b & 1 (other blocks still read p_old)
+  const int par = sc->body_runs & 1;
+  const CUtensorMap* pm = par ? &pm0 : &pm1;
+  const CUtensorMap* ph = par ? &ph0 : &ph1;
+  V* p_out = par ? p1 : p0;
+  TSeg seg[kTMaxSeg];
+  int nload = 0;
+  const int nseg = tsegments(NY / TY, NZ, seg, nload);
+  auto issue = [&](int l) {
+    int q = 0;
+    while(q + 1 < nseg && seg[q + 1].lbase <= l) ++q;
+    const int j0 = seg[q].tile * TY;
+    int jm, jp;
+    double sg;
+    nb_lo(j0, NY, o.periodic[1], o.dir_lo[1], jm, sg);
+    nb_hi(j0 + TY - 1, NY, o.periodic[1], o.dir_hi[1], jp, sg);
+    const int kz = vst::zrow(seg[q].kb - 1 + (l - seg[q].lbase), NZ, o.periodic[2], o.dir_lo[2],
+                             o.dir_hi[2], sg);
+    const int sl = l % D;
+    tma::mbar_arrive_expect_tx(&bars[sl], tx_bytes);
+    tma::load_3d(zslot(sl) + NX, &zm_, &bars[sl], 0, j0, kz);
+    tma::load_3d(zslot(sl), &zh, &bars[sl], 0, jm, kz);
+    tma::load_3d(zslot(sl) + (TY + 1) * NX, &zh, &bars[sl], 0, jp, kz);
+    tma::load_3d(pslot(sl) + NX, pm, &bars[sl], 0, j0, kz);
+    tma::load_3d(pslot(sl), ph, &bars[sl], 0, jm, kz);
+    tma::load_3d(pslot(sl) + (TY + 1) * NX, ph, &bars[sl], 0, jp, kz);
+  };
+  if(threadIdx.x == 0) {
+    for(int sl = 0; sl < D; ++sl) tma::mbar_init(&bars[sl], 1);
+    tma::fence_barrier_init();
+  }
+  __syncthreads();
+  int next = 0;
+  if(threadIdx.x == 0)
+    while(next < nload && next < D) issue(next++);
+  const int first = sc->first;
+  const double beta = first ? 0.0 : sc->beta;
+  const double sz = ls0->sx, spo = sc->sp;
+  const double alpha_old = sc->alpha, sx = sc->sx;
+  const double ix = o.inv2[0], iy = o.inv2[1], iz = o.inv2[2];
+  // raw operand z + beta p_old of the 4 cells at slot row fr
+  auto operand = [&](int sl, int fr, double (&v)[CPT]) {
+    double zv[CPT], pv[CPT];
+    tload4<double>(zslot(sl) + fr * NX + i0, zv);
+    tload4<double>(pslot(sl) + fr * NX + i0, pv);
+#pragma unroll
+    for(int t = 0; t < CPT; ++t) v[t] = zv[t] + beta * pv[t];
+  };
+  auto point = [&](int sl, int fr, int ii) {
+    return double(zslot(sl)[fr * NX + ii]) + beta * double(pslot(sl)[fr * NX + ii]);
+  };
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  int xl, xr;
+  double sxl, sxr;
+  nb_lo(i0, NX, o.periodic[0], o.dir_lo[0], xl, sxl);
+  nb_hi(i0 + CPT - 1, NX, o.periodic[0], o.dir_hi[0], xr, sxr);
+  for(int q = 0; q < nseg; ++q) {
+    const TSeg sg = seg[q];
+    const int j0 = sg.tile * TY;
+    const int j = j0 + r;
+    int jm, jp;
+    double sylo, syhi;
+    nb_lo(j0, NY, o.periodic[1], o.dir_lo[1], jm, sylo);
+    nb_hi(j0 + TY - 1, NY, o.periodic[1], o.dir_hi[1], jp, syhi);
+    auto own = [&](int l, double (&v)[CPT]) {
+      tma::mbar_wait(&bars[l % D], (l / D) & 1, fault, 1);
+      operand(l % D, r + 1, v);
+      if constexpr(!PER) {
+        double zs;
+        vst::zrow(sg.kb - 1 + (l - sg.lbase), NZ, o.periodic[2], o.dir_lo[2], o.dir_hi[2], zs);
+#pragma unroll
+        for(int t = 0; t < CPT; ++t) v[t] *= zs;
+      }
+    };
+    double below[CPT], cen[CPT], above[CPT];
+    own(sg.lbase, below);
+    own(sg.lbase + 1, cen);
+    // x of the own cells one plane ahead (plain loads, prefetched a step early)
+    double xn[CPT] = {0.0, 0.0, 0.0, 0.0};
+    if(!first) tload4<double>(x + o.L.idx(i0, j, sg.kb), xn);
+    __syncthreads();
+    for(int k = sg.kb; k < sg.ke; ++k) {
+      const int c = sg.lbase + 1 + (k - sg.kb);
+      if(threadIdx.x == 0) {
+        tma::fence_proxy_async();
+        while(next < nload && next <= c - 1 + D) issue(next++);
+      }
+      own(c + 1, above);
+      const int sl = c % D;
+      double dn[CPT], up[CPT];
+      operand(sl, r, dn);
+      operand(sl, r + 2, up);
+      double left = point(sl, r + 1, xl), right = point(sl, r + 1, xr);
+      if constexpr(!PER) {
+        const double sd = r == 0 ? sylo : 1.0, su = r == TY - 1 ? syhi : 1.0;
+#pragma unroll
+        for(int t = 0; t < CPT; ++t) {
+          dn[t] *= sd;
+          up[t] *= su;
+        }
+        left *= sxl;
+        right *= sxr;
+      }
+      // own cells: exact p (with shifts), the deferred x update
+      double zc[CPT], pc[CPT];
+      tload4<double>(zslot(sl) + (r + 1) * NX + i0, zc);
+      tload4<double>(pslot(sl) + (r + 1) * NX + i0, pc);
+      double pn[CPT], apv[CPT];
+#pragma unroll
+      for(int t = 0; t < CPT; ++t) {
+        const double l = t > 0 ? cen[t - 1] : left;
+        const double rr = t < CPT - 1 ? cen[t + 1] : right;
+        const double two_c = 2.0 * cen[t];
+        apv[t] = -(rr - two_c + l) * ix - (up[t] - two_c + dn[t]) * iy - (above[t] - two_c + below[t]) * iz;
+        pn[t] = first ? zc[t] - sz : (zc[t] - sz) + beta * (pc[t] - spo);
+      }
+      const size_t gq = o.L.idx(i0, j, k);
+      tstore4<V>(p_out + gq, pn);
+      tstore4<V>(ap + gq, apv);
+      if(!first) {
+        double xv[CPT];
+#pragma unroll
+        for(int t = 0; t < CPT; ++t) xv[t] = xn[t];
+        if(k + 1 < sg.ke) tload4<double>(x + o.L.idx(i0, j, k + 1), xn);
+#pragma unroll
+        for(int t = 0; t < CPT; ++t) {
+          xv[t] = (xv[t] - sx) + alpha_old * (pc[t] - spo);
+          acc[3] += xv[t];
+        }
+        tstore4<V>(x + gq, xv);
+      }
+#pragma unroll
+      for(int t = 0; t < CPT; ++t) {
+        acc[0] += pn[t];
+        acc[1] += apv[t];
+        acc[2] += pn[t] * apv[t];
+        below[t] = cen[t];
+        cen[t] = above[t];
+      }
+      __syncthreads();
+    }
+  }
+  const bool mx[4] = {false, false, false, false};
+  reduce_finish<4>(acc, mx, rb, [=](const Sums<4>& st) {
+    const int n = sc->n;
+    const int zmn = sc->zero_mean;
+    const double sp = zmn ? st.v[0] / n : 0.0;
+    const double sap = zmn ? st.v[1] / n : 0.0;
+    sc->sp = sp;
+    sc->sap = sap;
+    if(!first) sc->sx = zmn ? st.v[3] / n : 0.0;
+    sc->first = 0;
+    const double pap = st.v[2] - sp * st.v[1] - sap * st.v[0] + n * sp * sap;
+    sc->pap = pap;
+    if(fabs(pap) < kSmallNumber) {
+      sc->stop = 1;
+    } else {
+      sc->alpha = sc->rz / pap;
+    }
+  });
+}
+
+// r = (r - sr) - alpha (Ap - sap), its norm and the convergence test: the
+// residual half of k_update_xr for the fused CG step (x is updated one body
+// later by k_tpap, and after the loop by k_x_final).
+template <typename V>
+__global__ void __launch_bounds__(kTX* kTY)
+    k_update_r(CLay L, V* __restrict__ r, const V* __restrict__ ap, SolveScalars* sc, int kchunk,
+               RedBuf rb, cudaGraphConditionalHandle cond) {
+  STENCIL_PROLOGUE(L)
+  const int stop = sc->stop;
+  const double alpha = sc->alpha, sr = sc->sr, sap = sc->sap;
+  double acc[2];
+  zero(acc);
+  if(valid && !stop) {
+    for(int k = k0; k < k1; ++k) {
+      const int q = L.idx(i, j, k);
+      const double v = (double(r[q]) - sr) - alpha * (double(ap[q]) - sap);
+      r[q] = V(v);
+      acc[0] += v;
+      acc[1] += v * v;
+    }
+  }
+  const bool mx[2] = {false, false};
+  reduce_finish<2>(acc, mx, rb, [=](const Sums<2>& s) {
+    sc->body_runs += 1;
+    if(sc->stop) {
+      sc->cont = 0;
+      if(cond) cudaGraphSetConditional(cond, 0);
+      return;
+    }
+    const int n = sc->n;
+    const int zm = sc->zero_mean;
+    const double srn = zm ? s.v[0] / n : 0.0;
+    sc->sr = srn;
+    sc->sum_r = s.v[0];
+    const double ss = fmax(s.v[1] - n * srn * srn, 0.0);
+    sc->rnorm = sqrt(ss / n);
+    sc->iterations += 1;
+    sc->rel = sc->r0 > 0.0 ? sc->rnorm / sc->r0 : 0.0;
+    if(sc->rel <= sc->tol) sc->converged = 1;
+    if(sc->hist != nullptr && sc->iterations < sc->hist_cap) sc->hist[sc->iterations] = sc->rnorm;
+    sc->cont = (sc->converged || sc->iterations >= sc->max_it) ? 0 : 1;
+    if(cond) cudaGraphSetConditional(cond, sc->cont);
+  });
+}
+
+// After a fused-step loop: the last deferred update x = (x - sx) + alpha (p - sp)
+// unless the loop stopped on a vanishing p.Ap (then the reference skips it).
+template <typename V>
+__global__ void __launch_bounds__(kTX* kTY)
+    k_x_final(CLay L, V* __restrict__ x, const V* p0, const V* p1, SolveScalars* sc, int kchunk, RedBuf rb) {
+  STENCIL_PROLOGUE(L)
+  const int skip = sc->stop || sc->body_runs == 0;
+  const V* __restrict__ p = ((sc->body_runs - 1) & 1) ? p1 : p0;
+  const double alpha = sc->alpha, sx = sc->sx, sp = sc->sp;
+  double acc[1];
+  zero(acc);
+  if(valid && !skip) {
+    for(int k = k0; k < k1; ++k) {
+      const int q = L.idx(i, j, k);
+      const double v = (double(x[q]) - sx) + alpha * (double(p[q]) - sp);
+      x[q] = V(v);
+      acc[0] += v;
+    }
+  }
+  const bool mx[1] = {false};
+  reduce_finish<1>(acc, mx, rb, [=](const Sums<1>& s) {
+    if(!skip) sc->sx = sc->zero_mean ? s.v[0] / sc->n : 0.0;
+  });
+}
+
 // Residual + 2x2x2 restriction on the plane pipeline (same contract as
 // k_vrestrict): each step forms the residual (b - sb) - A (x - sx) on the two
 // fine planes of one coarse plane; a thread sums its cells pairwise in x and
@@ -2222,7 +2483,9 @@ struct PoissonPlan {
   int sms = 148;         // streaming multiprocessors of the plan's device
   bool tma_ap = false;   // plane-pipelined A p on the finest level
   bool all_periodic = false;  // every face periodic: constant diagonal, no boundary signs
-  CUtensorMap tm_pm, tm_ph;
+  CUtensorMap tm_pm, tm_ph, tm_pm2, tm_ph2;
+  double* p2 = nullptr;     // second p buffer of the fused CG step
+  float* p32b = nullptr;
   // levels tail_first.. run as one single-block launch (k_vcycle_tail)
   int tail_first = -1;
   TailArgs tail{};
@@ -2401,9 +2664,12 @@ void setup_tma(PoissonPlan* P, size_t tsz) {
     }
     if(l == 0) {
       const void* pp = P->precision == 1 ? static_cast<const void*>(P->p32) : P->p;
+      const void* pp2 = P->precision == 1 ? static_cast<const void*>(P->p32b) : P->p2;
       const int pes = P->precision == 1 ? 4 : 8;
       P->tm_pm = tma::make_map_3d(pp, pes, lv.L.nx, lv.L.ny, lv.L.nz, lv.L.nx, ty);
       P->tm_ph = tma::make_map_3d(pp, pes, lv.L.nx, lv.L.ny, lv.L.nz, lv.L.nx, 1);
+      P->tm_pm2 = tma::make_map_3d(pp2, pes, lv.L.nx, lv.L.ny, lv.L.nz, lv.L.nx, ty);
+      P->tm_ph2 = tma::make_map_3d(pp2, pes, lv.L.nx, lv.L.ny, lv.L.nz, lv.L.nx, 1);
       P->tma_ap = true;
     }
   }
@@ -2414,6 +2680,10 @@ void setup_tma(PoissonPlan* P, size_t tsz) {
   attr(reinterpret_cast<const void*>(k_tprolong<double, double, 4, 4, true>), tprolong_bytes<double, double>(256) * 4);
   attr(reinterpret_cast<const void*>(k_tprolong<float, float, 4, 4, false>), tprolong_bytes<float, float>(256) * 4);
   attr(reinterpret_cast<const void*>(k_tprolong<float, float, 4, 4, true>), tprolong_bytes<float, float>(256) * 4);
+  attr(reinterpret_cast<const void*>(k_tpap<double, double, false>), tround(6 * 256 * 8) * 2 * 4);
+  attr(reinterpret_cast<const void*>(k_tpap<double, double, true>), tround(6 * 256 * 8) * 2 * 4);
+  attr(reinterpret_cast<const void*>(k_tpap<float, float, false>), tround(6 * 256 * 4) * 2 * 4);
+  attr(reinterpret_cast<const void*>(k_tpap<float, float, true>), tround(6 * 256 * 4) * 2 * 4);
   attr(reinterpret_cast<const void*>(k_tap<double, 4, false>), tround(static_cast<size_t>(6) * 256 * 8) * kTSlots);
   attr(reinterpret_cast<const void*>(k_tap<double, 4, true>), tround(static_cast<size_t>(6) * 256 * 8) * kTSlots);
   attr(reinterpret_cast<const void*>(k_tap<float, 4, false>), tround(static_cast<size_t>(6) * 256 * 4) * kTSlots);
@@ -2567,15 +2837,17 @@ PoissonPlan* poisson_plan_create(const Grid& g, const PBC& pbc_in, int precision
   OFB_CHECK(cudaMalloc(&P->p, nf * sizeof(double)));
   OFB_CHECK(cudaMalloc(&P->ap, nf * sizeof(double)));
   OFB_CHECK(cudaMemset(P->p, 0, nf * sizeof(double)));
-  P->bytes += 5 * nf * sizeof(double);
+  OFB_CHECK(cudaMalloc(&P->p2, nf * sizeof(double)));
+  OFB_CHECK(cudaMemset(P->p2, 0, nf * sizeof(double)));
+  P->bytes += 6 * nf * sizeof(double);
   if(precision == 1) {
-    for(float** v : {&P->r32, &P->e32, &P->p32, &P->ap32}) {
+    for(float** v : {&P->r32, &P->e32, &P->p32, &P->ap32, &P->p32b}) {
       OFB_CHECK(cudaMalloc(v, nf * sizeof(float)));
       OFB_CHECK(cudaMemset(*v, 0, nf * sizeof(float)));
     }
     OFB_CHECK(cudaMalloc(&P->sc_in, sizeof(SolveScalars)));
     OFB_CHECK(cudaMemset(P->sc_in, 0, sizeof(SolveScalars)));
-    P->bytes += 4 * nf * sizeof(float);
+    P->bytes += 5 * nf * sizeof(float);
   }
   {
     int dev = 0;
@@ -2616,6 +2888,8 @@ void poisson_plan_destroy(PoissonPlan* P) {
   cudaFree(P->e32);
   cudaFree(P->p32);
   cudaFree(P->ap32);
+  cudaFree(P->p2);
+  cudaFree(P->p32b);
   cudaFree(P->sc_in);
   cudaFree(P->fault);
   delete P;
@@ -2818,10 +3092,10 @@ void v_cycle(PoissonPlan* P, int l, const V* r0, SolveScalars* sc, RedBuf rb, cu
 // inner solves of the mixed path's defect correction.
 template <typename V>
 struct CGVec {
-  V *b, *x, *r, *p, *ap;
+  V *b, *x, *r, *p, *ap, *p2;  // p2: the fused step's second p buffer
 };
 
-CGVec<double> cg64(PoissonPlan* P) { return CGVec<double>{P->b, P->x, P->r, P->p, P->ap}; }
+CGVec<double> cg64(PoissonPlan* P) { return CGVec<double>{P->b, P->x, P->r, P->p, P->ap, P->p2}; }
 
 // Initial residual and convergence test (linsolve/poisson_solver.cpp:717-739).
 template <typename V>
@@ -2832,6 +3106,26 @@ void enqueue_pre(PoissonPlan* P, const CGVec<V>& v, SolveScalars* sc, RedBuf rb,
   ProfScope ps(kKInitResidual, s);
   k_initial_residual<V><<<ln.grid, ln.block, 0, s>>>(l0.op, v.b, v.x, v.r, sc, ln.kchunk, rb, cond);
   OFB_LAUNCH_CHECK("k_initial_residual");
+}
+
+// The fused CG step needs the plane-pipeline maps of the finest level's
+// correction (z) and of p.  It is used for the FP32 inner solves of the mixed
+// path, where it is measurably faster; in FP64 the separate kernels are as
+// fast.  ORCHARD_B200_NO_VEC containing "fuse" keeps the separate kernels.
+bool fused_cg(const PoissonPlan* P) {
+  return P->precision == 1 && P->tma_ap && P->levels[0].tma_prolong && vec_enabled("tma") &&
+         vec_enabled("fuse");
+}
+
+// The last deferred x update of a fused-step loop.
+template <typename V>
+void enqueue_x_final(PoissonPlan* P, const CGVec<V>& v, SolveScalars* sc, RedBuf rb, cudaStream_t s) {
+  if(!fused_cg(P)) return;
+  const Level& l0 = P->levels[0];
+  const Launch3 ln = launch3(l0.L.nx, l0.L.ny, l0.L.nz);
+  ProfScope ps(kKUpdateXr, s);
+  k_x_final<V><<<ln.grid, ln.block, 0, s>>>(l0.L, v.x, v.p, v.p2, sc, ln.kchunk, rb);
+  OFB_LAUNCH_CHECK("k_x_final");
 }
 
 // One body of the rotated PCG loop: z = M r, p = z + beta p, A p, x/r update
@@ -2845,6 +3139,27 @@ void enqueue_body(PoissonPlan* P, const CGVec<V>& v, SolveScalars* sc, RedBuf rb
   const Level& l0 = P->levels[0];
   const Launch3 ln = launch3(l0.L.nx, l0.L.ny, l0.L.nz);
   v_cycle<T, V>(P, 0, v.r, sc, rb, s);
+  if(fused_cg(P)) {
+    // fused p update + A p + deferred x update, then the residual update
+    {
+      ProfScope ps(kKApplyAp, s);
+      const TGrid tg = tgrid(P, l0.L);
+      const size_t sm = (tround(static_cast<size_t>(tg.ty + 2) * l0.L.nx * sizeof(T)) +
+                         tround(static_cast<size_t>(tg.ty + 2) * l0.L.nx * sizeof(V))) * 4;
+      if(P->all_periodic)
+        k_tpap<T, V, true><<<tg.grid, 256, sm, s>>>(l0.op, l0.tm_xm, l0.tm_xh, P->tm_pm, P->tm_ph, P->tm_pm2,
+                                                    P->tm_ph2, P->ls, v.p, v.p2, v.ap, v.x, sc, rb, P->fault);
+      else
+        k_tpap<T, V, false><<<tg.grid, 256, sm, s>>>(l0.op, l0.tm_xm, l0.tm_xh, P->tm_pm, P->tm_ph, P->tm_pm2,
+                                                     P->tm_ph2, P->ls, v.p, v.p2, v.ap, v.x, sc, rb, P->fault);
+    }
+    {
+      ProfScope ps(kKUpdateXr, s);
+      k_update_r<V><<<ln.grid, ln.block, 0, s>>>(l0.L, v.r, v.ap, sc, ln.kchunk, rb, cond);
+    }
+    OFB_LAUNCH_CHECK("fused pcg body");
+    return;
+  }
   {
     ProfScope ps(kKUpdateP, s);
     k_update_p<T, V><<<ln.grid, ln.block, 0, s>>>(l0.L, static_cast<const T*>(l0.x), P->ls, v.p,
@@ -2962,6 +3277,7 @@ void solve_impl(PoissonPlan* P, int max_iterations, double tolerance, SolveScala
           [&](cudaGraphConditionalHandle c) { enqueue_body<T, double>(P, v, sc, rb, s, c); },
           &P->graph);
     OFB_CHECK(cudaGraphLaunch(P->exec, s));
+    enqueue_x_final<double>(P, v, sc, rb, s);
     OFB_CHECK(cudaMemcpyAsync(host, sc, sizeof(SolveScalars), cudaMemcpyDeviceToHost, s));
     OFB_CHECK(cudaStreamSynchronize(s));
     prof_add_counts(P->pre_counts, 1);
@@ -2977,6 +3293,10 @@ void solve_impl(PoissonPlan* P, int max_iterations, double tolerance, SolveScala
       OFB_CHECK(cudaStreamSynchronize(s));
       prof_collect();
     }
+    enqueue_x_final<double>(P, v, sc, rb, s);
+    OFB_CHECK(cudaMemcpyAsync(host, sc, sizeof(SolveScalars), cudaMemcpyDeviceToHost, s));
+    OFB_CHECK(cudaStreamSynchronize(s));
+    prof_collect();
   }
   if(history != nullptr && history_cap > 0) {
     const int n = std::min(history_cap, std::min(host->iterations + 1, P->hist_cap));
@@ -3020,7 +3340,7 @@ void solve_dc(PoissonPlan* P, int max_iterations, double tolerance, SolveScalars
   }
   OFB_CHECK(cudaMemcpyAsync(host, sc, sizeof(SolveScalars), cudaMemcpyDeviceToHost, s));
   OFB_CHECK(cudaStreamSynchronize(s));
-  const CGVec<float> v{nullptr, P->e32, P->r32, P->p32, P->ap32};
+  const CGVec<float> v{nullptr, P->e32, P->r32, P->p32, P->ap32, P->p32b};
   SolveScalars* si = P->sc_in;
   auto pre = [&](cudaGraphConditionalHandle c) {
     ProfScope ps(kKDefectCorrection, s);
@@ -3029,6 +3349,7 @@ void solve_dc(PoissonPlan* P, int max_iterations, double tolerance, SolveScalars
   };
   auto body = [&](cudaGraphConditionalHandle c) { enqueue_body<T, float>(P, v, si, rb, s, c); };
   auto post = [&]() {
+    enqueue_x_final<float>(P, v, si, rb, s);
     ProfScope ps(kKDefectCorrection, s, 2);
     k_dc_update_x<<<ln.grid, ln.block, 0, s>>>(l0.L, P->x, P->e32, sc, si, ln.kchunk, rb);
     k_dc_residual<<<ln.grid, ln.block, 0, s>>>(l0.op, P->b, P->x, P->r, sc, si, ln.kchunk, rb);
