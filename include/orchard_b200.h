@@ -160,6 +160,8 @@ of_status of_destroy(of_ctx* ctx);
 of_status of_set_precision(of_ctx* ctx, int precision);
 /* Bytes of device memory the context holds. */
 of_status of_device_bytes(of_ctx* ctx, size_t* bytes);
+/* The grid the context was created on. */
+of_status of_get_grid(of_ctx* ctx, of_grid* grid);
 
 /* ---- operator entry points (host buffers) ------------------------------- */
 
@@ -208,6 +210,34 @@ of_status of_state_download(of_ctx* ctx, double* u, double* v, double* w, double
  * v = -cos x sin y [cos z], p = +1/4 (cos 2x + cos 2y) [2D] or
  * +1/16 (cos 2x + cos 2y)(cos 2z + 2) [3D]. */
 of_status of_tg_init(of_ctx* ctx, double viscosity, double dt, int mode);
+
+/* Fluid at rest with the boundary conditions applied: zero velocity, history
+ * and total pressure, then the velocity ghost fills and the total-pressure
+ * ghosts from viscosity * Laplacian (initialize_lid_driven_cavity_state,
+ * solver/lid_driven_cavity.cpp:390-408).  Metrics reset, metrics.dt = dt. */
+of_status of_rest_init(of_ctx* ctx, double viscosity, double dt);
+
+/* ---- diagnostics of the resident state (case-driver validation) --------- */
+
+/* kinetic_energy (solver/taylor_green.cpp:269-289): the mean over cells of
+ * 1/2 |face-averaged velocity|^2, reduced on the device. */
+of_status of_kinetic_energy(of_ctx* ctx, double* energy);
+
+/* velocity_relative_l2_error (solver/taylor_green.cpp:291-333) of the
+ * resident velocity against the Taylor-Green field of phase `mode` (as
+ * of_tg_init) decayed by exp(-rate * viscosity * time), rate 3 in 3D and 2 in
+ * 2D; reduced on the device. */
+of_status of_tg_velocity_error(of_ctx* ctx, double viscosity, double time, int mode,
+                               double* error);
+
+/* Copies one storage line of a resident field to the host: field 0 = total
+ * pressure, 1..3 = velocity u, v, w; the line runs along `axis` (0..2) over
+ * the whole storage extent n of that axis, through the storage indices
+ * (i, j, k) of the other two axes (the index along `axis` is ignored).
+ * `out` holds n doubles; *n_out (optional) receives n.  The centreline
+ * samples of the cavity (solver/lid_driven_cavity.cpp:100-131) are such lines. */
+of_status of_sample_line(of_ctx* ctx, int field, int axis, int i, int j, int k, double* out,
+                         int* n_out);
 
 /* Runs `steps` projection steps on the resident state: the loop body of
  * run_taylor_green_steps (solver/taylor_green.cpp:577-633) and of

@@ -17,6 +17,8 @@
 #ifndef ORCHARD_ORACLE_H
 #define ORCHARD_ORACLE_H
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -198,6 +200,29 @@ double oo_cavity_dt(const oo_cavity_config* c);
 int oo_cavity_bc(const oo_cavity_config* c, oo_bc* bc);
 int oo_cavity_init(const oo_cavity_config* c, oo_state* s);
 int oo_cavity_steps(const oo_cavity_config* c, int steps, oo_state* s);
+
+/* ---- reference build only (oracle/_ref/liborchard_ref.so) -------------------
+ * The reference's drivers and I/O around the step, exported for the golden
+ * fixtures of the case layer: config files, describe(), the SLVCHKP1
+ * checkpoint, finalize and the VTK writer.  validate_* are the configs'
+ * boolean keys (they enter describe() and the checkpoint). */
+int oo_ref_tg_config_load(const char* path, oo_tg_config* c, int* validate_energy, char* describe,
+                          size_t cap);
+int oo_ref_cavity_config_load(const char* path, oo_cavity_config* c, int* validate_reference,
+                              char* describe, size_t cap);
+/* "name|version|compiler_id|compiler_version|profile|strict" of get_build_info. */
+int oo_ref_build_description(char* buf, size_t cap);
+int oo_ref_cavity_checkpoint_write(const char* path, const oo_cavity_config* c, int validate_reference,
+                                   const oo_state* s);
+/* meta[0..2] = checksum, build hash, configuration hash. */
+int oo_ref_cavity_checkpoint_load(const char* path, const oo_cavity_config* c, int validate_reference,
+                                  oo_state* s, unsigned long long meta[3]);
+/* finalize_lid_driven_cavity_result on a state: extrema (u max, u min, v max,
+ * v min), the four envelope samples and errors, the worst error and pass. */
+int oo_ref_cavity_finalize(const oo_cavity_config* c, int validate_reference, const oo_state* s,
+                           double extrema[4], double samples[4], double errors[4], double* max_error,
+                           int* pass);
+int oo_ref_write_vtk(const char* path, const oo_grid* g, const oo_state* s);
 
 #ifdef __cplusplus
 }

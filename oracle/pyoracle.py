@@ -322,6 +322,59 @@ class Oracle:
         return s
 
 
+class ReferenceIO(Oracle):
+    """The reference build's drivers and I/O around the step (config files,
+    describe, SLVCHKP1 checkpoint, finalize, VTK): liborchard_ref.so only."""
+
+    def __init__(self, path=REF_SO):
+        super().__init__(path)
+
+    def tg_config_load(self, path):
+        c, val, buf = TGConfig(), C.c_int(), C.create_string_buffer(4096)
+        self._check(self.lib.oo_ref_tg_config_load(str(path).encode(), C.byref(c), C.byref(val), buf,
+                                                   C.c_size_t(4096)))
+        return c, bool(val.value), buf.value.decode()
+
+    def cavity_config_load(self, path):
+        c, val, buf = CavityConfig(), C.c_int(), C.create_string_buffer(4096)
+        self._check(self.lib.oo_ref_cavity_config_load(str(path).encode(), C.byref(c), C.byref(val),
+                                                       buf, C.c_size_t(4096)))
+        return c, bool(val.value), buf.value.decode()
+
+    def build_description(self):
+        buf = C.create_string_buffer(1024)
+        self._check(self.lib.oo_ref_build_description(buf, C.c_size_t(1024)))
+        return buf.value.decode()
+
+    def cavity_checkpoint_write(self, path, cfg, validate_reference, s):
+        cs = s.to_c()
+        self._check(self.lib.oo_ref_cavity_checkpoint_write(str(path).encode(), C.byref(cfg),
+                                                            int(validate_reference), C.byref(cs)))
+
+    def cavity_checkpoint_load(self, path, cfg, validate_reference):
+        s = State.empty(self.cavity_grid(cfg))
+        cs = s.to_c()
+        meta = (C.c_ulonglong * 3)()
+        self._check(self.lib.oo_ref_cavity_checkpoint_load(str(path).encode(), C.byref(cfg),
+                                                           int(validate_reference), C.byref(cs), meta))
+        s.from_c(cs)
+        return s, {"checksum": meta[0], "build_hash": meta[1], "configuration_hash": meta[2]}
+
+    def cavity_finalize(self, cfg, validate_reference, s):
+        cs = s.to_c()
+        ext, smp, err = (C.c_double * 4)(), (C.c_double * 4)(), (C.c_double * 4)()
+        worst, ok = C.c_double(), C.c_int()
+        self._check(self.lib.oo_ref_cavity_finalize(C.byref(cfg), int(validate_reference), C.byref(cs),
+                                                    ext, smp, err, C.byref(worst), C.byref(ok)))
+        return {"u_vertical_max": ext[0], "u_vertical_min": ext[1], "v_horizontal_max": ext[2],
+                "v_horizontal_min": ext[3], "samples": list(smp), "errors": list(err),
+                "max_relative_error": worst.value, "pass": bool(ok.value)}
+
+    def write_vtk(self, path, grid, s):
+        cs = s.to_c()
+        self._check(self.lib.oo_ref_write_vtk(str(path).encode(), C.byref(grid), C.byref(cs)))
+
+
 def tg_config(nx, ny, nz, viscosity=0.01, cfl_limit=0.5, final_time=0.5,
               poisson_max_iterations=200, poisson_tolerance=1e-10):
     """TaylorGreenConfig with the reference's defaults (solver/taylor_green.hpp:18-30)."""

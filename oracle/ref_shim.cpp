@@ -7,6 +7,9 @@
 #include "orchard_oracle.h"
 
 #include "core/fields.hpp"
+#include "core/runtime.hpp"
+#include "io/checkpoint.hpp"
+#include "io/vtk_export.hpp"
 #include "linsolve/poisson_solver.hpp"
 #include "operators/discrete_operators.hpp"
 #include "solver/lid_driven_cavity.hpp"
@@ -14,6 +17,7 @@
 #include "solver/projection.hpp"
 #include "solver/taylor_green.hpp"
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <stdexcept>
@@ -499,6 +503,118 @@ int oo_cavity_steps(const oo_cavity_config* c, int steps, oo_state* s) {
     solver::run_lid_driven_cavity_steps(config, steps, st);
     store_state(st, s);
     store_metrics(st.metrics, s->metrics);
+  });
+}
+
+}  // extern "C"
+
+// ---- reference build only: drivers and I/O around the step ----------------
+
+namespace {
+
+void copy_text(char* dst, size_t cap, const std::string& text) {
+  if(dst == nullptr || cap == 0) return;
+  const size_t n = std::min(cap - 1, text.size());
+  std::memcpy(dst, text.data(), n);
+  dst[n] = '\0';
+}
+
+solver::LidDrivenCavityConfig make_cavity_full(const oo_cavity_config* c, int validate_reference) {
+  solver::LidDrivenCavityConfig config = make_cavity(c);
+  config.validate_reference = validate_reference != 0;
+  return config;
+}
+
+}  // namespace
+
+extern "C" {
+
+int oo_ref_tg_config_load(const char* path, oo_tg_config* c, int* validate_energy, char* describe,
+                          size_t cap) {
+  return guarded([&] {
+    const solver::TaylorGreenConfig config = solver::load_taylor_green_config(path);
+    *c = oo_tg_config{config.nx, config.ny, config.nz, config.viscosity, config.cfl_limit,
+                      config.final_time, config.poisson_max_iterations, config.poisson_tolerance};
+    if(validate_energy) *validate_energy = config.validate_energy ? 1 : 0;
+    copy_text(describe, cap, solver::describe(config));
+  });
+}
+
+int oo_ref_cavity_config_load(const char* path, oo_cavity_config* c, int* validate_reference,
+                              char* describe, size_t cap) {
+  return guarded([&] {
+    const solver::LidDrivenCavityConfig config = solver::load_lid_driven_cavity_config(path);
+    *c = oo_cavity_config{config.nx, config.ny, config.reynolds, config.lid_velocity, config.cfl_limit,
+                          config.max_steps, config.min_steps, config.steady_tolerance,
+                          config.poisson_max_iterations, config.poisson_tolerance};
+    if(validate_reference) *validate_reference = config.validate_reference ? 1 : 0;
+    copy_text(describe, cap, solver::describe(config));
+  });
+}
+
+int oo_ref_build_description(char* buf, size_t cap) {
+  return guarded([&] {
+    const solver::BuildInfo b = solver::get_build_info();
+    copy_text(buf, cap,
+              b.project_name + "|" + b.project_version + "|" + b.compiler_id + "|" + b.compiler_version +
+                  "|" + b.build_profile + "|" + (b.fast_math_enabled ? "fast-math" : "strict"));
+  });
+}
+
+int oo_ref_cavity_checkpoint_write(const char* path, const oo_cavity_config* c, int validate_reference,
+                                   const oo_state* s) {
+  return guarded([&] {
+    const solver::LidDrivenCavityConfig config = make_cavity_full(c, validate_reference);
+    solver::LidDrivenCavityState st(solver::make_lid_driven_cavity_grid(config));
+    load_state(st, s);
+    load_metrics(st.metrics, s->metrics);
+    solver::io::write_lid_driven_cavity_checkpoint(path, config, st);
+  });
+}
+
+int oo_ref_cavity_checkpoint_load(const char* path, const oo_cavity_config* c, int validate_reference,
+                                  oo_state* s, unsigned long long meta[3]) {
+  return guarded([&] {
+    const solver::LidDrivenCavityConfig config = make_cavity_full(c, validate_reference);
+    const solver::io::LidDrivenCavityCheckpoint ck = solver::io::load_lid_driven_cavity_checkpoint(path, config);
+    store_state(ck.state, s);
+    store_metrics(ck.state.metrics, s->metrics);
+    meta[0] = ck.metadata.checksum;
+    meta[1] = ck.metadata.build_hash;
+    meta[2] = ck.metadata.configuration_hash;
+  });
+}
+
+int oo_ref_cavity_finalize(const oo_cavity_config* c, int validate_reference, const oo_state* s,
+                           double extrema[4], double samples[4], double errors[4], double* max_error,
+                           int* pass) {
+  return guarded([&] {
+    const solver::LidDrivenCavityConfig config = make_cavity_full(c, validate_reference);
+    solver::LidDrivenCavityState st(solver::make_lid_driven_cavity_grid(config));
+    load_state(st, s);
+    load_metrics(st.metrics, s->metrics);
+    const solver::LidDrivenCavityResult r = solver::finalize_lid_driven_cavity_result(config, st);
+    extrema[0] = r.extrema.u_vertical_max;
+    extrema[1] = r.extrema.u_vertical_min;
+    extrema[2] = r.extrema.v_horizontal_max;
+    extrema[3] = r.extrema.v_horizontal_min;
+    for(int q = 0; q < 4; ++q) {
+      samples[q] = r.validation.points[q].sample_value;
+      errors[q] = r.validation.points[q].relative_error;
+    }
+    *max_error = r.validation.max_relative_error;
+    *pass = r.validation.pass ? 1 : 0;
+  });
+}
+
+int oo_ref_write_vtk(const char* path, const oo_grid* g, const oo_state* s) {
+  return guarded([&] {
+    const solver::Grid grid = make_grid(g);
+    solver::VelocityField velocity(grid);
+    solver::PressureField pressure(grid);
+    load_velocity(velocity, s->u, s->v, s->w);
+    load(pressure, s->p);
+    solver::io::write_mac_fields_vtk(path, velocity, pressure);
   });
 }
 

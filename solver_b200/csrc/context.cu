@@ -54,6 +54,11 @@ of_status guarded(Fn&& fn) {
 
 }  // namespace
 
+namespace ofb {
+// Lets the case layer (cases.cpp) report through of_last_error().
+void set_last_error(const std::string& message) { g_last_error = message; }
+}  // namespace ofb
+
 using ofb::Grid;
 using ofb::Lay;
 using ofb::PBC;
@@ -127,6 +132,7 @@ struct of_ctx {
   double* corrected[3] = {nullptr, nullptr, nullptr};
   double* prhs = nullptr;       // padded pressure rhs
   double* phi = nullptr;        // padded pressure correction (operator API)
+  double* diag = nullptr;       // diagnostics reductions (4 doubles)
 
   ofb::RedBuf rb{};
   ofb::SolveScalars* sc = nullptr;       // device
@@ -155,6 +161,7 @@ struct of_ctx {
     cudaFree(p_total);
     cudaFree(prhs);
     cudaFree(phi);
+    cudaFree(diag);
     cudaFree(rb.partials);
     cudaFree(rb.ticket);
     cudaFree(sc);
@@ -781,6 +788,14 @@ of_status of_set_precision(of_ctx* ctx, int precision) {
   });
 }
 
+of_status of_get_grid(of_ctx* ctx, of_grid* grid) {
+  return guarded([&] {
+    require_ctx(ctx);
+    require_ptr(grid, "grid");
+    *grid = of_grid{ctx->g.nx, ctx->g.ny, ctx->g.nz, ctx->g.dx, ctx->g.dy, ctx->g.dz};
+  });
+}
+
 of_status of_stream(of_ctx* ctx, void** stream) {
   return guarded([&] {
     require_ctx(ctx);
@@ -989,29 +1004,111 @@ of_status of_state_download(of_ctx* ctx, double* u, double* v, double* w, double
   });
 }
 
+namespace {
+
+// Shared tail of the initial states: zero every velocity-shaped buffer and the
+// total pressure, fill the analytic Taylor-Green field (mode 0/1) or leave the
+// fluid at rest (mode < 0), then the ghost fills of the reference's init
+// (solver/taylor_green.cpp:391-394, solver/lid_driven_cavity.cpp:401-406).
+void init_state(of_ctx* ctx, double viscosity, double dt, int mode) {
+  for(int c = 0; c < 3; ++c) {
+    double* bufs[6] = {ctx->vel[c], ctx->adv_prev[c], ctx->adv_cur[c],
+                       ctx->rhs[c], ctx->adi_b[c], ctx->corrected[c]};
+    for(double* b : bufs) OFB_CHECK(cudaMemsetAsync(b, 0, ctx->size(1 + c) * sizeof(double), ctx->stream));
+  }
+  OFB_CHECK(cudaMemsetAsync(ctx->p_total, 0, ctx->size(0) * sizeof(double), ctx->stream));
+  if(mode >= 0)
+    ofb::launch_tg_init(ctx->g, mode, ctx->vel[0], ctx->vel[1], ctx->vel[2], ctx->p_total, ctx->stream);
+  ofb::launch_velocity_bc(ctx->g, ctx->bc, ctx->vel[0], ctx->vel[1], ctx->vel[2], ctx->stream);
+  ofb::launch_total_pressure_bc(ctx->g, ctx->bc, viscosity, ctx->vel[0], ctx->vel[1], ctx->vel[2],
+                                ctx->p_total, ctx->stream);
+  ctx->has_prev = 0;
+  ctx->metrics = of_step_metrics{};
+  ctx->metrics.dt = dt;
+  ctx->state_clean = true;
+  ctx->sync();
+}
+
+// Device scratch of the diagnostics reductions (4 doubles), made on first use.
+double* diag_buffer(of_ctx* ctx) {
+  if(ctx->diag == nullptr) {
+    OFB_CHECK(cudaMalloc(&ctx->diag, 4 * sizeof(double)));
+    ctx->bytes += 4 * sizeof(double);
+  }
+  return ctx->diag;
+}
+
+}  // namespace
+
 of_status of_tg_init(of_ctx* ctx, double viscosity, double dt, int mode) {
   return guarded([&] {
     require_ctx(ctx);
     if(mode != 0 && mode != 1) fail(OF_INVALID_ARGUMENT, "Taylor-Green initial-state mode must be 0 or 1");
-    for(int c = 0; c < 3; ++c) {
-      OFB_CHECK(cudaMemsetAsync(ctx->vel[c], 0, ctx->size(1 + c) * sizeof(double), ctx->stream));
-      OFB_CHECK(cudaMemsetAsync(ctx->adv_prev[c], 0, ctx->size(1 + c) * sizeof(double), ctx->stream));
-      OFB_CHECK(cudaMemsetAsync(ctx->adv_cur[c], 0, ctx->size(1 + c) * sizeof(double), ctx->stream));
-      OFB_CHECK(cudaMemsetAsync(ctx->rhs[c], 0, ctx->size(1 + c) * sizeof(double), ctx->stream));
-      OFB_CHECK(cudaMemsetAsync(ctx->adi_b[c], 0, ctx->size(1 + c) * sizeof(double), ctx->stream));
-      OFB_CHECK(cudaMemsetAsync(ctx->corrected[c], 0, ctx->size(1 + c) * sizeof(double), ctx->stream));
-    }
-    OFB_CHECK(cudaMemsetAsync(ctx->p_total, 0, ctx->size(0) * sizeof(double), ctx->stream));
-    ofb::launch_tg_init(ctx->g, mode, ctx->vel[0], ctx->vel[1], ctx->vel[2], ctx->p_total, ctx->stream);
-    // initial-state tail (solver/taylor_green.cpp:391-394)
-    ofb::launch_velocity_bc(ctx->g, ctx->bc, ctx->vel[0], ctx->vel[1], ctx->vel[2], ctx->stream);
-    ofb::launch_total_pressure_bc(ctx->g, ctx->bc, viscosity, ctx->vel[0], ctx->vel[1], ctx->vel[2],
-                                  ctx->p_total, ctx->stream);
-    ctx->has_prev = 0;
-    ctx->metrics = of_step_metrics{};
-    ctx->metrics.dt = dt;
-    ctx->state_clean = true;
+    init_state(ctx, viscosity, dt, mode);
+  });
+}
+
+of_status of_rest_init(of_ctx* ctx, double viscosity, double dt) {
+  return guarded([&] {
+    require_ctx(ctx);
+    init_state(ctx, viscosity, dt, -1);
+  });
+}
+
+of_status of_kinetic_energy(of_ctx* ctx, double* energy) {
+  return guarded([&] {
+    require_ctx(ctx);
+    require_ptr(energy, "energy");
+    double* d = diag_buffer(ctx);
+    ofb::launch_kinetic_energy(ctx->g, ctx->vel[0], ctx->vel[1], ctx->vel[2], ctx->rb, d, ctx->stream);
+    double sum = 0.0;
+    OFB_CHECK(cudaMemcpyAsync(&sum, d, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     ctx->sync();
+    *energy = sum / static_cast<double>(ctx->lay[0].active_count());
+  });
+}
+
+of_status of_tg_velocity_error(of_ctx* ctx, double viscosity, double time, int mode, double* error) {
+  return guarded([&] {
+    require_ctx(ctx);
+    require_ptr(error, "error");
+    if(mode != 0 && mode != 1) fail(OF_INVALID_ARGUMENT, "Taylor-Green initial-state mode must be 0 or 1");
+    // exact_decay (solver/taylor_green.cpp:258-261)
+    const double rate = ctx->g.nz > 1 ? 3.0 : 2.0;
+    const double decay = std::exp(-rate * viscosity * time);
+    double* d = diag_buffer(ctx);
+    double num = 0.0, den = 0.0;
+    for(int c = 0; c < 3; ++c) {
+      ofb::launch_tg_error(ctx->g, 1 + c, mode, decay, ctx->vel[c], ctx->rb, d, ctx->stream);
+      double part[2];
+      OFB_CHECK(cudaMemcpyAsync(part, d, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+      ctx->sync();
+      num += part[0];
+      den += part[1];
+    }
+    *error = den > 0.0 ? std::sqrt(num / den) : std::sqrt(num);
+  });
+}
+
+of_status of_sample_line(of_ctx* ctx, int field, int axis, int i, int j, int k, double* out,
+                         int* n_out) {
+  return guarded([&] {
+    require_ctx(ctx);
+    require_ptr(out, "output line");
+    if(field < 0 || field > 3) fail(OF_INVALID_ARGUMENT, "field must be 0 (pressure) or 1..3 (velocity)");
+    if(axis < 0 || axis > 2) fail(OF_INVALID_ARGUMENT, "axis must be 0, 1 or 2");
+    const Lay& L = ctx->lay[field];
+    int idx[3] = {i, j, k};
+    idx[axis] = 0;
+    for(int a = 0; a < 3; ++a)
+      if(idx[a] < 0 || idx[a] >= L.s(a)) throw std::out_of_range("storage coordinate index outside field extent");
+    const double* base = field == 0 ? ctx->p_total : ctx->vel[field - 1];
+    const int n = L.s(axis);
+    const size_t stride = static_cast<size_t>(L.stride(axis)) * sizeof(double);
+    OFB_CHECK(cudaMemcpy2DAsync(out, sizeof(double), base + L.idx(idx[0], idx[1], idx[2]), stride,
+                                sizeof(double), n, cudaMemcpyDeviceToHost, ctx->stream));
+    ctx->sync();
+    if(n_out) *n_out = n;
   });
 }
 

@@ -191,6 +191,15 @@ void launch_dot_active(const Grid& g, int loc, const double* a, const double* b,
 // Geometry of one ADI sweep (begin, unknowns) for the viscosity derivative.
 void adi_axis_geometry(const AdiPlan* p, int comp, int axis, int* begin, int* n);
 
+// ---- validation reductions of the case drivers (diagnostics.cu) ----
+// out[0] = sum over cells of 1/2 |face-averaged velocity|^2.
+void launch_kinetic_energy(const Grid& g, const double* u, const double* v, const double* w,
+                           RedBuf rb, double* out, cudaStream_t s);
+// out[0] = sum (f - exact)^2, out[1] = sum exact^2 over the active entries of
+// the face field at `loc`, exact = the Taylor-Green state of phase `mode` x decay.
+void launch_tg_error(const Grid& g, int loc, int mode, double decay, const double* f, RedBuf rb,
+                     double* out, cudaStream_t s);
+
 // ---- allocation-free pressure rhs (noalloc.cu) ----
 // Device address of the file-scope scratch on the current device (looked up
 // once per device with cudaGetSymbolAddress, then cached).

@@ -1,5 +1,5 @@
-"""The C-ABI library: it loads, exports every entry point include/orchard_b200.h
-declares, and refuses to run without a GPU (there is no CPU fallback)."""
+"""The C-ABI library: it loads, exports every entry point include/*.h declares,
+and refuses to run without a GPU (there is no CPU fallback)."""
 import os
 import re
 import subprocess
@@ -7,14 +7,17 @@ import subprocess
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-HEADER = os.path.join(ROOT, "include", "orchard_b200.h")
+HEADERS = [os.path.join(ROOT, "include", h) for h in ("orchard_b200.h", "orchard_b200_cases.h")]
 LIB = os.path.join(ROOT, "solver_b200", "liborchard_b200.so")
 
 
 def declared_symbols():
-    text = open(HEADER).read()
-    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    return sorted(set(re.findall(r"\b(of_[a-z0-9_]+)\s*\(", text)))
+    names = set()
+    for header in HEADERS:
+        text = open(header).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names |= set(re.findall(r"\b(of_[a-z0-9_]+)\s*\(", text))
+    return sorted(names)
 
 
 def test_library_exports_every_declared_symbol():
@@ -25,7 +28,10 @@ def test_library_exports_every_declared_symbol():
     missing = [s for s in declared_symbols() if s not in exported]
     assert not missing, missing
     import solver_b200._capi as capi
+    import solver_b200.cases as cases
     assert set(capi.EXPORTED_SYMBOLS) <= exported
+    assert set(cases.CASE_SYMBOLS) <= exported
+    assert set(declared_symbols()) <= set(capi.EXPORTED_SYMBOLS) | set(cases.CASE_SYMBOLS)
 
 
 def test_library_loads_and_reports_abi_version():
@@ -40,3 +46,6 @@ def test_no_cpu_fallback_without_gpu():
     import solver_b200 as sb
     with pytest.raises(sb.OfError, match="no CUDA device"):
         sb.Context(sb.Grid(4, 4, 4, 1.0, 1.0, 1.0), [sb.PERIODIC] * 6)
+    import solver_b200.cases as cases
+    with pytest.raises(sb.OfError, match="no CUDA device"):
+        cases.TaylorGreenCase(cases.TaylorGreenConfig(nx=8, ny=8))
