@@ -87,6 +87,11 @@ def bytes_per_launch(n, precision):
         "cell_pass": 7 * d * N,
     }
     if precision == "mixed":
+        # the FP32 inner CG fuses the p update, A p and the deferred x update
+        # into one plane-pipelined launch (read z, p_old, x; write p, A p, x)
+        # and updates r alone (read r, A p; write r)
+        out["pcg_apply_ap"] = 6 * s * N
+        out["pcg_update_xr"] = 3 * s * N
         out["defect_correction"] = 20 * N
     return out
 
@@ -101,7 +106,8 @@ def read_peaks():
 
 
 def read_traffic():
-    """Per-launch DRAM bytes from the committed ncu summary (profiles/)."""
+    """Per-launch DRAM bytes of kernel classes (FP64, 256^3) from the committed
+    ncu summary (profiles/ncu_traffic.txt)."""
     p = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
     out = {}
     if os.path.exists(p):
@@ -356,7 +362,8 @@ def run_b200_arm(args, world, rank, local):
     avg_s = dom_ms / dom_timed / 1000.0
     achieved = bpl[dom] / avg_s / 1e9
     peak, peak_kind = read_peaks()
-    traffic = read_traffic().get(dom)
+    # the committed ncu figures are for the FP64 256^3 workload
+    traffic = read_traffic().get(dom) if (args.precision == "fp64" and n == 256) else None
     step_bytes = sum(bpl[k] * v[0] for k, v in prof.items() if k in bpl) / replay_steps
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                 "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,

@@ -271,49 +271,6 @@ struct SweepArgs {
   const double* z;
 };
 
-__global__ void __launch_bounds__(128) k_adi_sweep(SweepArgs a, const double* __restrict__ in,
-                                                   double* __restrict__ out) {
-  const Lay& L = a.L;
-  const int axis = a.axis;
-  const int a1 = axis == 0 ? 1 : 0;
-  const int a2 = axis == 2 ? 1 : 2;
-  const int t1 = blockIdx.x * blockDim.x + threadIdx.x;
-  const int t2 = blockIdx.y;
-  if(t1 >= L.n(a1) || t2 >= L.n(a2)) return;
-  int c[3] = {0, 0, 0};
-  c[a1] = t1 + 1;
-  c[a2] = t2 + 1;
-  const int base = L.idx(c[0], c[1], c[2]);
-  const int st = L.stride(axis);
-  const int n = a.n;
-  const double* __restrict__ src = in + base + a.begin * st;
-  double* __restrict__ dst = out + base + a.begin * st;
-  // forward elimination
-  double r = src[0] + a.rhs_first;
-  if(n == 1) r += a.rhs_last;
-  double m = r * __ldg(&a.ip[0]);
-  dst[0] = m;
-  for(int q = 1; q < n; ++q) {
-    double rq = src[q * st];
-    if(q == n - 1) rq += a.rhs_last;
-    m = (rq - a.lower * m) * __ldg(&a.ip[q]);
-    dst[q * st] = m;
-  }
-  // back substitution
-  const double x_last = m;
-  double x = m;
-  for(int q = n - 2; q >= 0; --q) {
-    x = dst[q * st] - __ldg(&a.cu[q]) * x;
-    dst[q * st] = x;
-  }
-  if(a.periodic && n > 1) {
-    // Sherman-Morrison update (solver/projection.cpp:607-616)
-    const double factor = (x + a.uc_over_gamma * x_last) * a.inv_den;
-    for(int q = 0; q < n; ++q) dst[q * st] -= factor * __ldg(&a.z[q]);
-  }
-  if(a.copy_duplicate) out[base + a.dup_index * st] = dst[0];
-}
-
 // Shared-memory line solver: one warp stages `lines` whole lines in shared
 // memory (coalesced: x-lines load row segments, y/z-lines load 32 adjacent
 // i-lines so each warp load is one contiguous row), solves them there with

@@ -1,7 +1,7 @@
-// Momentum-side stencils: the fused predictor right-hand side (TVD/van Leer
-// advection, diffusion, pressure gradient, factorisation correction and the
-// AB2 combination in one pass), the stand-alone advection operator and the
-// Taylor-Green initial state.
+// Momentum-side stencils: the TVD/van Leer advection term (one launch per
+// component), the rest of the predictor right-hand side (diffusion, pressure
+// gradient, factorisation correction and the AB2 combination in one pass)
+// and the Taylor-Green initial state.
 #include "kernels.hpp"
 
 namespace ofb {
@@ -9,17 +9,6 @@ namespace ofb {
 namespace {
 
 constexpr double kSmallDenominator = 1.0e-14;  // solver/momentum_terms.cpp:14
-
-__device__ __forceinline__ double van_leer(double r) {
-  // limiter_value (solver/momentum_terms.cpp:26-33)
-  const double a = fabs(r);
-  return (r + a) / (1.0 + a);
-}
-
-__device__ __forceinline__ double safe_ratio(double num, double den) {
-  // solver/momentum_terms.cpp:35-40
-  return fabs(den) < kSmallDenominator ? 0.0 : num / den;
-}
 
 // Branch-free form of one reconstruct_face call: every candidate value is
 // loaded before the velocity sign is known and the reference's three cases
@@ -30,6 +19,7 @@ __device__ __forceinline__ double tvd_face(double vel, double left, double right
   const bool up = vel >= 0.0;
   const double delta = right - left;
   const double num = up ? left - far_left : far_right - right;
+  // safe_ratio and limiter_value (solver/momentum_terms.cpp:26-40)
   const double ratio = fabs(delta) < kSmallDenominator ? 0.0 : num / delta;
   const double a = fabs(ratio);
   const double phi = (ratio + a) / (1.0 + a);

@@ -328,7 +328,7 @@ __global__ void __launch_bounds__(kTX* kTY)
 // ---------------------------------------------------------------------------
 
 template <typename T>
-__host__ __device__ __forceinline__ bool vfits(const CLay& L) {
+inline bool vfits(const CLay& L) {
   return vst::row_fits(L.nx, vst::Width<T>::W);
 }
 
@@ -743,7 +743,6 @@ __global__ void k_coarse_solve(int n, const int* __restrict__ swaps, const doubl
 // nx is 64, 128 or 256 and TY divides ny.
 // ---------------------------------------------------------------------------
 constexpr int kTSlots = 5;
-constexpr int kTThreads = 256;
 
 __host__ __device__ inline size_t tround(size_t b) { return (b + 127) / 128 * 128; }
 
