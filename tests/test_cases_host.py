@@ -296,3 +296,24 @@ def test_checkpoint_round_trip_with_library_hash(tmp_path):
     assert meta["build_hash"] == cs.library_build_hash()
     for k in ("u", "v", "w", "adv_u", "adv_v", "adv_w", "p"):
         assert np.array_equal(loaded[k], state[k])
+
+
+CONFIGS = os.path.join(os.path.dirname(HERE), "solver_b200", "configs")
+
+
+@pytest.mark.parametrize("name,steps", [("taylor_green_2d_128.cfg", 100), ("taylor_green_3d_256.cfg", 200)])
+def test_shipped_taylor_green_configs(refio, name, steps):
+    path = os.path.join(CONFIGS, name)
+    ours = cs.load_taylor_green_config(path)
+    _, _, text = refio.tg_config_load(path)
+    assert cs.describe(ours) == text
+    assert cs.taylor_green_case(ours)[3] == steps
+
+
+@pytest.mark.parametrize("name", ["lid_driven_cavity_re100_128.cfg", "lid_driven_cavity_re100_1024.cfg"])
+def test_shipped_cavity_configs(refio, name):
+    path = os.path.join(CONFIGS, name)
+    ours = cs.load_lid_driven_cavity_config(path)
+    _, _, text = refio.cavity_config_load(path)
+    assert cs.describe(ours) == text
+    assert ours.steady_tolerance == 1e-8 and ours.reynolds == 100.0
