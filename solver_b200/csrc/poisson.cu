@@ -1495,6 +1495,13 @@ __global__ void __launch_bounds__(1024 / CPT)
 // is z + beta p_old: the operator annihilates the mean shifts wherever they
 // are nonzero (periodic / all-Neumann problems).  Records sp, sap, pap and
 // alpha as k_update_p and k_apply_ap do, and mean(x).
+// Ring depth of k_tpap: its registers allow two blocks per SM, so FP32
+// planes (half the bytes) get twice the slots to keep as many bytes in flight.
+template <typename V>
+constexpr int tpap_slots() {
+  return 4;
+}
+
 template <typename T, typename V, bool PER>
 __global__ void __launch_bounds__(256)
     k_tpap(OpInfo o, const __grid_constant__ CUtensorMap zm_, const __grid_constant__ CUtensorMap zh,
@@ -1503,7 +1510,7 @@ __global__ void __launch_bounds__(256)
            const LevelScalars* ls0, V* p0, V* p1, V* __restrict__ ap, V* __restrict__ x,
            SolveScalars* sc, RedBuf rb, int* fault) {
   constexpr int CPT = 4;
-  constexpr int D = 4;
+  constexpr int D = tpap_slots<V>();
   extern __shared__ __align__(128) unsigned char tsm[];
   __shared__ uint64_t bars[D];
   const int NX = o.L.nx, NY = o.L.ny, NZ = o.L.nz;
@@ -1681,19 +1688,69 @@ __global__ void __launch_bounds__(256)
 
 // r = (r - sr) - alpha (Ap - sap), its norm and the convergence test: the
 // residual half of k_update_xr for the fused CG step (x is updated one body
-// later by k_tpap, and after the loop by k_x_final).
+// later by k_tpap, and after the loop by k_x_final).  The compact vector is
+// one contiguous array, so it is swept flat, 16 bytes per load (float4 /
+// double2) with kFlatUnroll loads of each operand in flight per thread.
+constexpr int kFlatUnroll = 4;
+constexpr int kFlatThreads = 256;
+
 template <typename V>
-__global__ void __launch_bounds__(kTX* kTY)
-    k_update_r(CLay L, V* __restrict__ r, const V* __restrict__ ap, SolveScalars* sc, int kchunk,
-               RedBuf rb, cudaGraphConditionalHandle cond) {
-  STENCIL_PROLOGUE(L)
+struct Vec16;
+template <>
+struct Vec16<float> {
+  using T = float4;
+  static constexpr int W = 4;
+};
+template <>
+struct Vec16<double> {
+  using T = double2;
+  static constexpr int W = 2;
+};
+
+template <typename V>
+__global__ void __launch_bounds__(kFlatThreads)
+    k_update_r_flat(int n, V* __restrict__ r, const V* __restrict__ ap, SolveScalars* sc, RedBuf rb,
+                    cudaGraphConditionalHandle cond) {
+  using VT = typename Vec16<V>::T;
+  constexpr int W = Vec16<V>::W;
   const int stop = sc->stop;
   const double alpha = sc->alpha, sr = sc->sr, sap = sc->sap;
   double acc[2];
   zero(acc);
-  if(valid && !stop) {
-    for(int k = k0; k < k1; ++k) {
-      const int q = L.idx(i, j, k);
+  if(!stop) {
+    const int nv = n / W;
+    const int stride = gridDim.x * blockDim.x;
+    VT* rv = reinterpret_cast<VT*>(r);
+    const VT* av = reinterpret_cast<const VT*>(ap);
+    for(int base = blockIdx.x * blockDim.x + threadIdx.x; base < nv; base += kFlatUnroll * stride) {
+      VT rr[kFlatUnroll], aa[kFlatUnroll];
+#pragma unroll
+      for(int u = 0; u < kFlatUnroll; ++u) {
+        const int q = base + u * stride;
+        if(q < nv) {
+          rr[u] = rv[q];
+          aa[u] = av[q];
+        }
+      }
+#pragma unroll
+      for(int u = 0; u < kFlatUnroll; ++u) {
+        const int q = base + u * stride;
+        if(q < nv) {
+          V* rs = reinterpret_cast<V*>(&rr[u]);
+          const V* as = reinterpret_cast<const V*>(&aa[u]);
+#pragma unroll
+          for(int w = 0; w < W; ++w) {
+            const double v = (double(rs[w]) - sr) - alpha * (double(as[w]) - sap);
+            rs[w] = V(v);
+            acc[0] += v;
+            acc[1] += v * v;
+          }
+          rv[q] = rr[u];
+        }
+      }
+    }
+    // the n % W elements past the last full vector
+    for(int q = nv * W + blockIdx.x * blockDim.x + threadIdx.x; q < n; q += stride) {
       const double v = (double(r[q]) - sr) - alpha * (double(ap[q]) - sap);
       r[q] = V(v);
       acc[0] += v;
@@ -1708,13 +1765,13 @@ __global__ void __launch_bounds__(kTX* kTY)
       if(cond) cudaGraphSetConditional(cond, 0);
       return;
     }
-    const int n = sc->n;
+    const int nn = sc->n;
     const int zm = sc->zero_mean;
-    const double srn = zm ? s.v[0] / n : 0.0;
+    const double srn = zm ? s.v[0] / nn : 0.0;
     sc->sr = srn;
     sc->sum_r = s.v[0];
-    const double ss = fmax(s.v[1] - n * srn * srn, 0.0);
-    sc->rnorm = sqrt(ss / n);
+    const double ss = fmax(s.v[1] - nn * srn * srn, 0.0);
+    sc->rnorm = sqrt(ss / nn);
     sc->iterations += 1;
     sc->rel = sc->r0 > 0.0 ? sc->rnorm / sc->r0 : 0.0;
     if(sc->rel <= sc->tol) sc->converged = 1;
@@ -2681,8 +2738,8 @@ void setup_tma(PoissonPlan* P, size_t tsz) {
   attr(reinterpret_cast<const void*>(k_tprolong<float, float, 4, 4, true>), tprolong_bytes<float, float>(256) * 4);
   attr(reinterpret_cast<const void*>(k_tpap<double, double, false>), tround(6 * 256 * 8) * 2 * 4);
   attr(reinterpret_cast<const void*>(k_tpap<double, double, true>), tround(6 * 256 * 8) * 2 * 4);
-  attr(reinterpret_cast<const void*>(k_tpap<float, float, false>), tround(6 * 256 * 4) * 2 * 4);
-  attr(reinterpret_cast<const void*>(k_tpap<float, float, true>), tround(6 * 256 * 4) * 2 * 4);
+  attr(reinterpret_cast<const void*>(k_tpap<float, float, false>), tround(6 * 256 * 4) * 2 * tpap_slots<float>());
+  attr(reinterpret_cast<const void*>(k_tpap<float, float, true>), tround(6 * 256 * 4) * 2 * tpap_slots<float>());
   attr(reinterpret_cast<const void*>(k_tap<double, 4, false>), tround(static_cast<size_t>(6) * 256 * 8) * kTSlots);
   attr(reinterpret_cast<const void*>(k_tap<double, 4, true>), tround(static_cast<size_t>(6) * 256 * 8) * kTSlots);
   attr(reinterpret_cast<const void*>(k_tap<float, 4, false>), tround(static_cast<size_t>(6) * 256 * 4) * kTSlots);
@@ -2935,10 +2992,26 @@ struct TGrid {
   int grid, ty;
 };
 
-TGrid tgrid(const PoissonPlan* P, const CLay& L) {
+// Blocks per SM of the plane-pipeline kernels: two for 8-byte data (the ring
+// of a 256-wide level then holds ~100 KB per block); four for 4-byte data,
+// whose planes carry half the bytes, so that each SM keeps as many bytes in
+// flight (measured: the FP32 V-cycle kernels 18-22 % faster than at two).
+int tper_sm(size_t elem) { return elem == 8 ? 2 : 4; }
+
+// Blocks of one plane-pipeline launch: tper_sm blocks per SM, no more than
+// fit on an SM at once (the persistent schedule gives every block an equal
+// share), at least 4 tile-planes per block.
+int resident_blocks(const void* kernel, size_t smem) {
+  int n = 0;
+  OFB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, 256, smem));
+  return std::max(1, n);
+}
+
+TGrid tgrid(const PoissonPlan* P, const CLay& L, size_t elem, const void* kernel, size_t smem) {
   const int ty = 1024 / L.nx;
   const long long items = static_cast<long long>(L.ny / ty) * L.nz;
-  long long g = std::min<long long>(2LL * P->sms, std::max(1LL, items / 4));
+  const int per_sm = std::min(tper_sm(elem), resident_blocks(kernel, smem));
+  long long g = std::min<long long>(static_cast<long long>(per_sm) * P->sms, std::max(1LL, items / 4));
   while((items / g + 1) / L.nz + 2 > kTMaxSeg) ++g;
   return TGrid{static_cast<int>(g), ty};
 }
@@ -2987,14 +3060,10 @@ void v_cycle(PoissonPlan* P, int l, const V* r0, SolveScalars* sc, RedBuf rb, cu
     const vst::RowLaunch lr = vst::row_launch(lv.L.nx, lv.L.ny, lv.L.nz, vst::Width<T>::W, 16);
     if(lv.tma && vec_enabled("tma")) {
       ProfScope ps(fine ? kKSmoothFirstFine : kKCoarseLevels, s);
-      const TGrid tg = tgrid(P, lv.L);
-      const size_t sm = tround(static_cast<size_t>(tg.ty + 2) * lv.L.nx * sizeof(B)) * kTSlots;
-      if(P->all_periodic)
-        k_tsmooth_pre<T, B, 4, true><<<tg.grid, 256, sm, s>>>(lv.op, lv.tm_bm, lv.tm_bh, sb_ptr, x, ls, zm, rb,
-                                                              P->fault);
-      else
-        k_tsmooth_pre<T, B, 4, false><<<tg.grid, 256, sm, s>>>(lv.op, lv.tm_bm, lv.tm_bh, sb_ptr, x, ls, zm,
-                                                               rb, P->fault);
+      const size_t sm = tround(static_cast<size_t>(1024 / lv.L.nx + 2) * lv.L.nx * sizeof(B)) * kTSlots;
+      const auto kern = P->all_periodic ? k_tsmooth_pre<T, B, 4, true> : k_tsmooth_pre<T, B, 4, false>;
+      const TGrid tg = tgrid(P, lv.L, sizeof(T), reinterpret_cast<const void*>(kern), sm);
+      kern<<<tg.grid, 256, sm, s>>>(lv.op, lv.tm_bm, lv.tm_bh, sb_ptr, x, ls, zm, rb, P->fault);
     } else if(vsm && vec_enabled("pre")) {
       ProfScope ps(fine ? kKSmoothFirstFine : kKCoarseLevels, s);
       k_vsmooth_pre<T, B><<<lr.grid, lr.block, 0, s>>>(lv.op, bptr, sb_ptr, x, ls, zm, lr.kchunk, rb);
@@ -3015,17 +3084,13 @@ void v_cycle(PoissonPlan* P, int l, const V* r0, SolveScalars* sc, RedBuf rb, cu
       ProfScope ps(fine ? kKRestrictFine : kKCoarseLevels, s);
       const int ty = 1024 / lv.L.nx;
       const long long items = static_cast<long long>(lv.L.ny / ty) * (lv.L.nz / 2);
-      long long g = std::min<long long>(2LL * P->sms, std::max(1LL, items / 2));
-      while((items / g + 1) / (lv.L.nz / 2) + 2 > kTMaxSeg) ++g;
       const size_t sm = tslot_bytes<T, B>(lv.L.nx) * kTSlots + static_cast<size_t>(ty) * (lv.L.nx / 2) * sizeof(T);
-      if(P->all_periodic)
-        k_trestrict<T, B, kTSlots, true><<<static_cast<int>(g), 256, sm, s>>>(
-            lv.op, cv.op, lv.tm_xm, lv.tm_xh, lv.tm_bm, sb_ptr, &ls->sx, static_cast<T*>(cv.b), lsc, zm, rb,
-            P->fault);
-      else
-        k_trestrict<T, B, kTSlots, false><<<static_cast<int>(g), 256, sm, s>>>(
-            lv.op, cv.op, lv.tm_xm, lv.tm_xh, lv.tm_bm, sb_ptr, &ls->sx, static_cast<T*>(cv.b), lsc, zm, rb,
-            P->fault);
+      const auto kern = P->all_periodic ? k_trestrict<T, B, kTSlots, true> : k_trestrict<T, B, kTSlots, false>;
+      const int per_sm = std::min(tper_sm(sizeof(T)), resident_blocks(reinterpret_cast<const void*>(kern), sm));
+      long long g = std::min<long long>(static_cast<long long>(per_sm) * P->sms, std::max(1LL, items / 2));
+      while((items / g + 1) / (lv.L.nz / 2) + 2 > kTMaxSeg) ++g;
+      kern<<<static_cast<int>(g), 256, sm, s>>>(lv.op, cv.op, lv.tm_xm, lv.tm_xh, lv.tm_bm, sb_ptr, &ls->sx,
+                                                static_cast<T*>(cv.b), lsc, zm, rb, P->fault);
     } else {
       ProfScope ps(fine ? kKRestrictFine : kKCoarseLevels, s);
       if(vre && lv.rx == 2 && lv.ry == 2 && lv.rz == 2) {
@@ -3042,15 +3107,11 @@ void v_cycle(PoissonPlan* P, int l, const V* r0, SolveScalars* sc, RedBuf rb, cu
     v_cycle<T, V>(P, l + 1, r0, sc, rb, s);
     if(lv.tma_prolong && vec_enabled("tma")) {
       ProfScope ps(fine ? kKProlongFine : kKCoarseLevels, s);
-      const TGrid tg = tgrid(P, lv.L);
-      if(P->all_periodic)
-        k_tprolong<T, B, 4, 4, true><<<tg.grid, 256, tprolong_bytes<T, B>(lv.L.nx) * 4, s>>>(
-            lv.op, lv.tm_xm, lv.tm_xh, lv.tm_bm, lv.tm_em, lv.tm_eh, sb_ptr, &ls->sx, &lsc->sx, a, ls, zm,
-            rb, P->fault);
-      else
-        k_tprolong<T, B, 4, 4, false><<<tg.grid, 256, tprolong_bytes<T, B>(lv.L.nx) * 4, s>>>(
-            lv.op, lv.tm_xm, lv.tm_xh, lv.tm_bm, lv.tm_em, lv.tm_eh, sb_ptr, &ls->sx, &lsc->sx, a, ls, zm,
-            rb, P->fault);
+      const size_t sm = tprolong_bytes<T, B>(lv.L.nx) * 4;
+      const auto kern = P->all_periodic ? k_tprolong<T, B, 4, 4, true> : k_tprolong<T, B, 4, 4, false>;
+      const TGrid tg = tgrid(P, lv.L, sizeof(T), reinterpret_cast<const void*>(kern), sm);
+      kern<<<tg.grid, 256, sm, s>>>(lv.op, lv.tm_xm, lv.tm_xh, lv.tm_bm, lv.tm_em, lv.tm_eh, sb_ptr, &ls->sx,
+                                    &lsc->sx, a, ls, zm, rb, P->fault);
     } else {
       ProfScope ps(fine ? kKProlongFine : kKCoarseLevels, s);
       if(vpr)
@@ -3064,14 +3125,11 @@ void v_cycle(PoissonPlan* P, int l, const V* r0, SolveScalars* sc, RedBuf rb, cu
     }
     if(lv.tma && vec_enabled("tma")) {
       ProfScope ps(fine ? kKSmoothFine : kKCoarseLevels, s);
-      const TGrid tg = tgrid(P, lv.L);
       const size_t sm = tslot_bytes<T, B>(lv.L.nx) * kTSlots;
-      if(P->all_periodic)
-        k_tsmooth<T, B, 4, true><<<tg.grid, 256, sm, s>>>(lv.op, lv.tm_am, lv.tm_ah, lv.tm_bm, sb_ptr, &ls->sa,
-                                                          x, ls, zm, rz_sc, rb, P->fault);
-      else
-        k_tsmooth<T, B, 4, false><<<tg.grid, 256, sm, s>>>(lv.op, lv.tm_am, lv.tm_ah, lv.tm_bm, sb_ptr,
-                                                           &ls->sa, x, ls, zm, rz_sc, rb, P->fault);
+      const auto kern = P->all_periodic ? k_tsmooth<T, B, 4, true> : k_tsmooth<T, B, 4, false>;
+      const TGrid tg = tgrid(P, lv.L, sizeof(T), reinterpret_cast<const void*>(kern), sm);
+      kern<<<tg.grid, 256, sm, s>>>(lv.op, lv.tm_am, lv.tm_ah, lv.tm_bm, sb_ptr, &ls->sa, x, ls, zm, rz_sc, rb,
+                                    P->fault);
     } else {
       ProfScope ps(fine ? kKSmoothFine : kKCoarseLevels, s);
       if(vsm)
@@ -3142,19 +3200,20 @@ void enqueue_body(PoissonPlan* P, const CGVec<V>& v, SolveScalars* sc, RedBuf rb
     // fused p update + A p + deferred x update, then the residual update
     {
       ProfScope ps(kKApplyAp, s);
-      const TGrid tg = tgrid(P, l0.L);
-      const size_t sm = (tround(static_cast<size_t>(tg.ty + 2) * l0.L.nx * sizeof(T)) +
-                         tround(static_cast<size_t>(tg.ty + 2) * l0.L.nx * sizeof(V))) * 4;
-      if(P->all_periodic)
-        k_tpap<T, V, true><<<tg.grid, 256, sm, s>>>(l0.op, l0.tm_xm, l0.tm_xh, P->tm_pm, P->tm_ph, P->tm_pm2,
-                                                    P->tm_ph2, P->ls, v.p, v.p2, v.ap, v.x, sc, rb, P->fault);
-      else
-        k_tpap<T, V, false><<<tg.grid, 256, sm, s>>>(l0.op, l0.tm_xm, l0.tm_xh, P->tm_pm, P->tm_ph, P->tm_pm2,
-                                                     P->tm_ph2, P->ls, v.p, v.p2, v.ap, v.x, sc, rb, P->fault);
+      const int ty = 1024 / l0.L.nx;
+      const size_t sm = (tround(static_cast<size_t>(ty + 2) * l0.L.nx * sizeof(T)) +
+                         tround(static_cast<size_t>(ty + 2) * l0.L.nx * sizeof(V))) * tpap_slots<V>();
+      const auto kern = P->all_periodic ? k_tpap<T, V, true> : k_tpap<T, V, false>;
+      const TGrid tg = tgrid(P, l0.L, sizeof(V), reinterpret_cast<const void*>(kern), sm);
+      kern<<<tg.grid, 256, sm, s>>>(l0.op, l0.tm_xm, l0.tm_xh, P->tm_pm, P->tm_ph, P->tm_pm2, P->tm_ph2, P->ls,
+                                    v.p, v.p2, v.ap, v.x, sc, rb, P->fault);
     }
     {
       ProfScope ps(kKUpdateXr, s);
-      k_update_r<V><<<ln.grid, ln.block, 0, s>>>(l0.L, v.r, v.ap, sc, ln.kchunk, rb, cond);
+      const int n = l0.L.count();
+      const int blocks = static_cast<int>(std::min<long long>(
+          kTargetBlocks, std::max(1LL, (static_cast<long long>(n) + kFlatThreads - 1) / kFlatThreads)));
+      k_update_r_flat<V><<<blocks, kFlatThreads, 0, s>>>(n, v.r, v.ap, sc, rb, cond);
     }
     OFB_LAUNCH_CHECK("fused pcg body");
     return;
@@ -3167,12 +3226,10 @@ void enqueue_body(PoissonPlan* P, const CGVec<V>& v, SolveScalars* sc, RedBuf rb
   {
     ProfScope ps(kKApplyAp, s);
     if(P->tma_ap && vec_enabled("tma")) {
-      const TGrid tg = tgrid(P, l0.L);
-      const size_t sm = tround(static_cast<size_t>(tg.ty + 2) * l0.L.nx * sizeof(V)) * kTSlots;
-      if(P->all_periodic)
-        k_tap<V, 4, true><<<tg.grid, 256, sm, s>>>(l0.op, P->tm_pm, P->tm_ph, v.ap, sc, rb, P->fault);
-      else
-        k_tap<V, 4, false><<<tg.grid, 256, sm, s>>>(l0.op, P->tm_pm, P->tm_ph, v.ap, sc, rb, P->fault);
+      const size_t sm = tround(static_cast<size_t>(1024 / l0.L.nx + 2) * l0.L.nx * sizeof(V)) * kTSlots;
+      const auto kern = P->all_periodic ? k_tap<V, 4, true> : k_tap<V, 4, false>;
+      const TGrid tg = tgrid(P, l0.L, sizeof(V), reinterpret_cast<const void*>(kern), sm);
+      kern<<<tg.grid, 256, sm, s>>>(l0.op, P->tm_pm, P->tm_ph, v.ap, sc, rb, P->fault);
     } else if(vfits<V>(l0.L) && vec_enabled() && vec_enabled("ap")) {
       const vst::RowLaunch lr = vst::row_launch(l0.L.nx, l0.L.ny, l0.L.nz, vst::Width<V>::W, 16);
       k_vapply_ap<V><<<lr.grid, lr.block, 0, s>>>(l0.op, v.p, v.ap, sc, lr.kchunk, rb);
