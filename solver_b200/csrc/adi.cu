@@ -29,11 +29,12 @@ struct AdiAxis {
   double uc_over_gamma = 0.0;
   double inv_den = 0.0;
   size_t off = 0;           // offset of cu/ip/z in the coefficient buffer
-  // partition (SPIKE) solver, used when n is a multiple of 32 and >= 64:
+  // partition (warp-scan) solver, used when 64 <= n <= 1024 (n a multiple of
+  // 32 on periodic axes; wall lines are padded to a multiple of 32):
   // per-lane segment factors, spikes and the interface operator, all laid
   // out [element][lane] so that a warp reads them with one coalesced load
   bool partition = false;
-  int seg = 0;              // K = n / 32
+  int seg = 0;              // K = ceil(n / 32)
   size_t poff = 0;          // offset: cu[K][32], ip[K][32], v[K][32], w[K][32], gl[64][32], gr[64][32]
 };
 
@@ -179,14 +180,18 @@ AdiPlan* adi_plan_create(const Grid& g, const VBC& bc, double alpha) {
       host.insert(host.end(), cu.begin(), cu.end());
       host.insert(host.end(), ip.begin(), ip.end());
       host.insert(host.end(), z.begin(), z.end());
-      if(n % 32 == 0 && n >= 64 && n / 32 <= 16) {
+      if(n >= 64 && (n + 31) / 32 <= 32 && (n % 32 == 0 || !periodic)) {
         // Warp-scan form of the two Thomas recurrences (lane p owns the
         // unknowns q = pK + j, j < K):
         //   forward  m_q = ip_q r_q + f_q m_{q-1},  f_q = -lower ip_q
         //   backward x_q = m_q + g_q x_{q+1},       g_q = -cu_q
         // Lane-local products of f (resp. g) and the per-step multipliers of
-        // the Kogge-Stone scans are line-independent and stored here.
-        const int P = 32, K = n / 32;
+        // the Kogge-Stone scans are line-independent and stored here.  A line
+        // whose n is not a multiple of 32 (walls) is padded to 32 K unknowns
+        // with ip = cu = 0: the padding decouples (m = x = 0 there) and the
+        // real unknowns are unchanged.  Periodic lines are not padded (the
+        // Sherman-Morrison update reads the last unknown from lane 31).
+        const int P = 32, K = (n + 31) / 32;
         std::vector<double> fB(K * P), gD(K * P), ipj(K * P), cuj(K * P), zj(K * P);
         std::vector<double> mf(5 * P, 0.0), mb(5 * P, 0.0);
         std::vector<double> lane_f(P), lane_g(P);
@@ -194,18 +199,19 @@ AdiPlan* adi_plan_create(const Grid& g, const VBC& bc, double alpha) {
           double prod = 1.0;
           for(int j = 0; j < K; ++j) {
             const int q = lane * K + j;
-            const double f = q == 0 ? 0.0 : -(-beta) * ip[q];
+            const double ipq = q < n ? ip[q] : 0.0;
+            const double f = q == 0 ? 0.0 : -(-beta) * ipq;
             prod = j == 0 ? f : prod * f;
             fB[j * P + lane] = prod;
-            ipj[j * P + lane] = ip[q];
-            cuj[j * P + lane] = cu[q];
-            zj[j * P + lane] = z[q];
+            ipj[j * P + lane] = ipq;
+            cuj[j * P + lane] = q < n ? cu[q] : 0.0;
+            zj[j * P + lane] = q < n ? z[q] : 0.0;
           }
           lane_f[lane] = prod;  // m_end = A + prod * m_in
           double dprod = 1.0;
           for(int j = K - 1; j >= 0; --j) {
             const int q = lane * K + j;
-            const double g = -cu[q];
+            const double g = q < n ? -cu[q] : 0.0;
             dprod = j == K - 1 ? g : dprod * g;
             gD[j * P + lane] = dprod;
           }
@@ -398,7 +404,7 @@ struct ScanArgs {
   int K;
 };
 
-// Warp-scan line solver: a block of 16 warps stages 16 lines in shared
+// Warp-scan line solver: a block of LB warps stages LB lines in shared
 // memory (element q = pK + j of a line at [j][p], so a warp's accesses are
 // conflict-free); warp w solves line w.  Lane p evaluates its K forward
 // elimination steps as an affine map of the unknown carried in from lane p-1,
@@ -407,11 +413,10 @@ struct ScanArgs {
 // (solver/projection.cpp:607-616) follows.  Same Thomas factors as the
 // reference's recurrences; the association of the products differs, so
 // results agree to rounding.
-template <bool XLINES>
-__global__ void __launch_bounds__(512) k_adi_scan(SweepArgs a, ScanArgs sa,
-                                                  const double* __restrict__ in,
-                                                  double* __restrict__ out) {
-  constexpr int LB = 16;
+template <bool XLINES, int LB>
+__global__ void __launch_bounds__(32 * LB) k_adi_scan(SweepArgs a, ScanArgs sa,
+                                                      const double* __restrict__ in,
+                                                      double* __restrict__ out) {
   extern __shared__ double tile[];
   const Lay& L = a.L;
   const int axis = a.axis;
@@ -419,7 +424,7 @@ __global__ void __launch_bounds__(512) k_adi_scan(SweepArgs a, ScanArgs sa,
   const int a2 = axis == 2 ? 1 : 2;
   const int n = a.n;
   const int K = sa.K;
-  const int S = n + 1;  // per-line stride in the tile
+  const int S = 32 * K + 1;  // per-line stride in the tile (n padded to 32 K)
   const int st = L.stride(axis);
   const int n1 = L.n(a1), n2 = L.n(a2);
   const int tid = threadIdx.x + 32 * threadIdx.y;
@@ -443,17 +448,18 @@ __global__ void __launch_bounds__(512) k_adi_scan(SweepArgs a, ScanArgs sa,
     return L.idx(c[0], c[1], c[2]) + a.begin * st;
   };
   auto slot = [&](int l, int q) { return l * S + (q % K) * 32 + q / K; };
+  // staged lines; the padding past n is zero
   if(XLINES) {
     bool ok;
     const int base = line_base(wl, ok);
     if(ok)
-      for(int q = lane; q < n; q += 32) tile[slot(wl, q)] = in[base + q];
+      for(int q = lane; q < 32 * K; q += 32) tile[slot(wl, q)] = q < n ? in[base + q] : 0.0;
   } else {
     const int l = tid % LB;
     bool ok;
     const int base = line_base(l, ok);
     if(ok)
-      for(int q = tid / LB; q < n; q += 512 / LB) tile[slot(l, q)] = in[base + q * st];
+      for(int q = tid / LB; q < 32 * K; q += 32) tile[slot(l, q)] = q < n ? in[base + q * st] : 0.0;
   }
   __syncthreads();
   {
@@ -526,9 +532,28 @@ __global__ void __launch_bounds__(512) k_adi_scan(SweepArgs a, ScanArgs sa,
     bool ok;
     const int base = line_base(l, ok);
     if(ok) {
-      for(int q = tid / LB; q < n; q += 512 / LB) out[base + q * st] = tile[slot(l, q)];
+      for(int q = tid / LB; q < n; q += 32) out[base + q * st] = tile[slot(l, q)];
       if(a.copy_duplicate && tid < LB) out[base - a.begin * st + a.dup_index * st] = tile[slot(l, 0)];
     }
+  }
+}
+
+template <int LB>
+void launch_scan(const SweepArgs& a, const ScanArgs& sa, int axis, int a1, int a2, const double* in,
+                 double* out, cudaStream_t s) {
+  const size_t smem = static_cast<size_t>(LB) * (32 * sa.K + 1) * sizeof(double);
+  const dim3 block(32, LB, 1);
+  if(axis == 0) {
+    const long long nl = static_cast<long long>(a.L.n(a1)) * a.L.n(a2);
+    const dim3 grid(static_cast<unsigned>((nl + LB - 1) / LB), 1, 1);
+    OFB_CHECK(cudaFuncSetAttribute(k_adi_scan<true, LB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(smem)));
+    k_adi_scan<true, LB><<<grid, block, smem, s>>>(a, sa, in, out);
+  } else {
+    const dim3 grid((a.L.n(a1) + LB - 1) / LB, a.L.n(a2), 1);
+    OFB_CHECK(cudaFuncSetAttribute(k_adi_scan<false, LB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(smem)));
+    k_adi_scan<false, LB><<<grid, block, smem, s>>>(a, sa, in, out);
   }
 }
 
@@ -569,20 +594,13 @@ void launch_adi_sweep(const AdiPlan* p, int comp, int axis, const double* in, do
     sa.z = base + 4 * KP;
     sa.mf = base + 5 * KP;
     sa.mb = base + 5 * KP + 5 * 32;
-    const size_t smem = static_cast<size_t>(16) * (a.n + 1) * sizeof(double);
-    dim3 block(32, 16, 1);
-    if(axis == 0) {
-      const long long nl = static_cast<long long>(a.L.n(a1)) * a.L.n(a2);
-      dim3 grid(static_cast<unsigned>((nl + 15) / 16), 1, 1);
-      OFB_CHECK(cudaFuncSetAttribute(k_adi_scan<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(smem)));
-      k_adi_scan<true><<<grid, block, smem, s>>>(a, sa, in, out);
-    } else {
-      dim3 grid((a.L.n(a1) + 15) / 16, a.L.n(a2), 1);
-      OFB_CHECK(cudaFuncSetAttribute(k_adi_scan<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(smem)));
-      k_adi_scan<false><<<grid, block, smem, s>>>(a, sa, in, out);
-    }
+    // 16 lines per block; 4 when that leaves fewer than two blocks per SM
+    // (few long lines, e.g. a 2D sweep)
+    const long long nl = static_cast<long long>(a.L.n(a1)) * a.L.n(a2);
+    if((nl + 15) / 16 >= 2LL * 148)
+      launch_scan<16>(a, sa, axis, a1, a2, in, out, s);
+    else
+      launch_scan<4>(a, sa, axis, a1, a2, in, out, s);
     OFB_LAUNCH_CHECK("k_adi_scan");
     return;
   }

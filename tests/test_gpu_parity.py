@@ -132,6 +132,28 @@ def test_predictor_adi_partition_solver_matches_oracle(sb, oracle, types):
         assert rel_maxdiff(a, b) <= OP_TOL
 
 
+@pytest.mark.parametrize("shape", [(200, 130, 1), (1000, 40, 1), (96, 70, 12)])
+def test_predictor_adi_padded_wall_lines_match_oracle(sb, oracle, shape):
+    """Wall lines whose length is not a multiple of 32 (199, 999, 95 ...
+    unknowns) take the warp-scan solver padded to a multiple of 32; few long
+    lines (2D) use blocks of four lines."""
+    rng = np.random.default_rng(9)
+    nx, ny, nz = shape
+    g = po.Grid(nx, ny, nz, 1.0 / nx, 1.0 / ny, 1.0 if nz == 1 else 1.0 / nz)
+    types = [po.NO_SLIP_WALL, po.NO_SLIP_WALL, po.NO_SLIP_WALL, po.PRESCRIBED_VELOCITY, po.SYMMETRY,
+             po.SYMMETRY]
+    vel = [None] * 6
+    vel[3] = (1.0, 0.0, 0.0)
+    bc = po.bc_from(types, vel)
+    rhs = _random_velocity(g, rng)
+    ctx = sb.Context(to_gpu_grid(g), to_gpu_bc(bc))
+    got, lines = ctx.solve_predictor_adi(rhs, 0.5 * 0.01 * 0.5 / (nx + ny))
+    exp, lines_ref = oracle.predictor_adi(g, bc, 0.5 * 0.01 * 0.5 / (nx + ny), *rhs)
+    assert lines == lines_ref
+    for a, b in zip(got, exp):
+        assert rel_maxdiff(a, b) <= OP_TOL
+
+
 @pytest.mark.parametrize("case", ["dirichlet2d", "neumann2d", "periodic3d", "mixed3d",
                                   "mixed3d_tiled"])
 def test_poisson_matches_oracle(sb, oracle, case):
