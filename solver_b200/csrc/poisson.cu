@@ -2992,11 +2992,11 @@ struct TGrid {
   int grid, ty;
 };
 
-// Blocks per SM of the plane-pipeline kernels: two for 8-byte data (the ring
-// of a 256-wide level then holds ~100 KB per block); four for 4-byte data,
-// whose planes carry half the bytes, so that each SM keeps as many bytes in
-// flight (measured: the FP32 V-cycle kernels 18-22 % faster than at two).
-int tper_sm(size_t elem) { return elem == 8 ? 2 : 4; }
+// Blocks per SM of the plane-pipeline kernels: four, or as many as fit (the
+// rings of the FP64 kernels on a 256-wide level hold ~100 KB, so two of
+// those; the lighter A p ring and the FP32 kernels, whose planes carry half
+// the bytes, fit three or four and keep more bytes in flight per SM).
+int tper_sm(size_t) { return 4; }
 
 // Blocks of one plane-pipeline launch: tper_sm blocks per SM, no more than
 // fit on an SM at once (the persistent schedule gives every block an equal
