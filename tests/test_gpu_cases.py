@@ -271,3 +271,30 @@ def test_case_rejects_mismatched_state_grid():
         with pytest.raises(ValueError, match="lid-driven cavity state grid does not match the config"):
             case._c = other.to_c()
             case.run_case_steps(1)
+
+
+def _cell_velocity(st):
+    """Cell-centred velocity of a 2D state, as the VTK export averages it."""
+    u, v = st["u"][1, 1:-1, :], st["v"][1, :, 1:-1]
+    uc = 0.5 * (u[:, 1:-2] + u[:, 2:-1])
+    vc = 0.5 * (v[1:-2, :] + v[2:-1, :])
+    return np.concatenate([uc.ravel(), vc.ravel()])
+
+
+def test_taylor_green_temporal_self_convergence_gate():
+    """The reference's temporal gate (validation/run_validation_suite.py:297-345,
+    501-502): Taylor-Green 128^2 to t = 0.25 at CFL 1, 0.5 and 0.25; the
+    observed order log2(|u1 - u2| / |u2 - u3|) of the final cell velocities
+    must be >= 1.8, and every run keeps div u at the 1e-10 mass gate."""
+    fields = []
+    for cfl in (1.0, 0.5, 0.25):
+        cfg = cs.TaylorGreenConfig(nx=128, ny=128, nz=1, viscosity=0.01, cfl_limit=cfl, final_time=0.25,
+                                   poisson_max_iterations=200, poisson_tolerance=1e-10)
+        with cs.TaylorGreenCase(cfg) as case:
+            r = case.run()
+            fields.append(_cell_velocity(case.download_state()))
+        assert r["final_step"]["max_divergence_l2"] <= 1e-10
+    d01 = np.linalg.norm(fields[0] - fields[1]) / np.linalg.norm(fields[1])
+    d12 = np.linalg.norm(fields[1] - fields[2]) / np.linalg.norm(fields[2])
+    order = math.log2(d01 / d12)
+    assert order >= 1.8, (d01, d12, order)
