@@ -317,3 +317,33 @@ def test_shipped_cavity_configs(refio, name):
     _, _, text = refio.cavity_config_load(path)
     assert cs.describe(ours) == text
     assert ours.steady_tolerance == 1e-8 and ours.reynolds == 100.0
+
+
+BIN = os.path.join(os.path.dirname(HERE), "solver_b200", "bin")
+
+CLI_CASES = [
+    ("solver_cavity", ["--foo"]),
+    ("solver_cavity", ["/nonexistent/cavity.cfg"]),
+    ("solver_cavity", ["--steps"]),
+    ("solver_cavity", ["a.cfg", "b.cfg"]),
+    ("solver_taylor_green", ["--vtk-out"]),
+    ("solver_taylor_green", ["--bogus", "x"]),
+    ("solver_taylor_green", ["/nonexistent/tg.cfg"]),
+]
+
+
+@pytest.mark.parametrize("tool,args", CLI_CASES)
+def test_cli_argument_errors_match_reference(tool, args):
+    """Argument and config errors of the CLIs come before any device work, so
+    they are compared with the reference's CLIs on the CPU: same stderr line,
+    same exit status."""
+    import subprocess
+    ref = os.path.join(os.path.dirname(po.REF_SO), tool)
+    ours = os.path.join(BIN, tool)
+    if not os.path.exists(ref):
+        pytest.skip("reference CLIs (oracle/_ref) not built")
+    a = subprocess.run([ours, *args], capture_output=True, text=True, timeout=60)
+    b = subprocess.run([ref, *args], capture_output=True, text=True, timeout=60)
+    assert a.returncode == b.returncode == 1
+    assert a.stderr == b.stderr
+    assert a.stdout == b.stdout == ""
