@@ -485,7 +485,7 @@ def mixed_extra(n, dt, args, fp64_value, error_steps=200):
               for c in "uvw") / max(float(np.max(np.abs(ref[c][1:-1, 1:-1, 1:-1]))) for c in "uvw")
     out["rel_velocity_error_vs_fp64"] = err
     out["error_steps"] = error_steps
-    out["precision"] = "FP32 V-cycle (storage and arithmetic) inside the FP64 CG"
+    out["precision"] = "FP64 defect correction (residual, update, convergence, mean removal) around an FP32 MG-PCG (V-cycle and CG vectors: FP32 storage and arithmetic)"
     return out
 
 
