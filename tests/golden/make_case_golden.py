@@ -11,7 +11,12 @@ reference itself (its sources compiled in place by ``make -C oracle ref``).
   reference's build description, checkpoint hashes and finalize outputs on
   that state, and ``cavity_24.vtk`` the reference's write_mac_fields_vtk of it.
 
-Usage:  make -C oracle ref && python tests/golden/make_case_golden.py
+* ``ref_cli_cavity_128_steady.txt`` (only with ``--with-steady``, about a
+  quarter of an hour of CPU): the reference's ``solver_cavity`` report for
+  the shipped config solver_b200/configs/lid_driven_cavity_re100_128.cfg,
+  marched to the steady state.
+
+Usage:  make -C oracle ref && python tests/golden/make_case_golden.py [--with-steady]
 """
 import json
 import os
@@ -55,9 +60,9 @@ validate_reference = true
 CAVITY_STEPS = 60
 
 
-def run_cli(binary, *args):
+def run_cli(binary, *args, cwd=OUT):
     p = subprocess.run([os.path.join(ROOT, "oracle", "_ref", binary), *args], capture_output=True,
-                       text=True, cwd=OUT)
+                       text=True, cwd=cwd)
     return p.stdout
 
 
@@ -98,6 +103,11 @@ def main():
     }
     with open(os.path.join(OUT, "cavity_24.json"), "w") as f:
         json.dump(info, f, indent=1, sort_keys=True)
+    if "--with-steady" in sys.argv:
+        report = run_cli("solver_cavity", os.path.join("solver_b200", "configs",
+                                                       "lid_driven_cavity_re100_128.cfg"), cwd=ROOT)
+        with open(os.path.join(OUT, "ref_cli_cavity_128_steady.txt"), "w") as f:
+            f.write(report)
     print("wrote", sorted(os.listdir(OUT)))
 
 

@@ -298,3 +298,42 @@ def test_taylor_green_temporal_self_convergence_gate():
     d12 = np.linalg.norm(fields[1] - fields[2]) / np.linalg.norm(fields[2])
     order = math.log2(d01 / d12)
     assert order >= 1.8, (d01, d12, order)
+
+
+def test_shipped_cavity_128_config_steady_like_the_reference():
+    """solver_b200/configs/lid_driven_cavity_re100_128.cfg (Re 100, max |du| <=
+    1e-8, Poisson tolerance 1e-8): the reference's build reaches the steady
+    state at step 9760 and passes the envelope gate; the device run must stop
+    within a step of it and pass too."""
+    root = os.path.dirname(HERE)
+    cfg = cs.load_lid_driven_cavity_config(
+        os.path.join(root, "solver_b200", "configs", "lid_driven_cavity_re100_128.cfg"))
+    with cs.LidDrivenCavityCase(cfg) as case:
+        r = case.run()
+    assert abs(r["final_step"]["step"] - 9760) <= 1, r["final_step"]
+    assert r["final_step"]["max_velocity_change"] <= 1e-8
+    assert r["pass"]
+
+
+def test_cavity_128_cli_report_to_steady_state_matches_reference():
+    """`solver_cavity` on the shipped 128^2 config, run to the steady state,
+    against the reference CLI's report for the same file: same step count
+    (within one), same gate verdict, centreline numbers to the printed
+    digits."""
+    gold = os.path.join(GOLD, "ref_cli_cavity_128_steady.txt")
+    if not os.path.exists(gold):
+        pytest.skip("steady-state fixture not generated (make_case_golden.py --with-steady)")
+    root = os.path.dirname(HERE)
+    exe = os.path.join(BIN, "solver_cavity")
+    p = subprocess.run([exe, os.path.join("solver_b200", "configs", "lid_driven_cavity_re100_128.cfg")],
+                       capture_output=True, text=True, cwd=root, timeout=600)
+    with open(gold) as f:
+        theirs = _report(f.read())
+    ours = _report(p.stdout)
+    assert p.returncode == 0, p.stderr
+    assert ours["config"] == theirs["config"] and ours["config_path"] == theirs["config_path"]
+    assert abs(int(ours["steps"]) - int(theirs["steps"])) <= 1
+    assert ours["benchmark_status"] == theirs["benchmark_status"] == "pass"
+    for k in ("u_vertical_max", "u_vertical_min", "v_horizontal_max", "v_horizontal_min",
+              "max_reference_relative_error"):
+        assert _same_number(ours[k], theirs[k], rel=2e-5), (k, ours[k], theirs[k])
