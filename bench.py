@@ -24,6 +24,11 @@ difference from the FP64 path after 200 steps; "adjoint" -- the adjoint check
 workload (128^3, nu = 0.01, perturbed Taylor-Green, 100 steps, checkpoint
 every 10): adjoint/forward device-time ratio and a central-difference check.
 
+``--adjoint-long`` runs, instead of the step benchmark, the long-horizon
+adjoint workload (512^3, Re 1600, 400 steps, mixed forward and adjoint with
+the binomial checkpoint schedule sized to the device memory; the gradient's
+mixed-vs-FP64 error checked at 256^3) and prints its own JSON line.
+
 Multi-GPU: the path does not shard (replicas only): each rank runs its own
 independent 256^3 simulation; value = total steps/s over ranks, time = max
 over ranks.
@@ -392,12 +397,10 @@ def run_b200_arm(args, world, rank, local):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
+    pinned["has_previous_advection"] = 1
+    pinned["metrics"] = st["metrics"]
     for _ in range(e2e_steps):
-        ctx.upload_state(pinned["u"], pinned["v"], pinned["w"], pinned["adv_u"], pinned["adv_v"],
-                         pinned["adv_w"], pinned["p"], 1, st["metrics"])
-        ctx.run_steps(prm, 1)
-        out = ctx.download_state_into(pinned)
-        st["metrics"] = out
+        ctx.step_host(prm, pinned)
     e1.record(stream)
     e1.synchronize()
     barrier()
@@ -419,8 +422,8 @@ def run_b200_arm(args, world, rank, local):
         "step_hbm": step_hbm,
         "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": state_bytes,
                 "d2h_bytes_per_step": state_bytes,
-                "note": "per step: state upload from pinned host memory, one step, state download "
-                        "(the C-ABI call a host-resident caller makes)"},
+                "note": "per step: of_step_host on pinned host state (upload, one step, download; "
+                        "the AB2 history is copied back while the pressure solve runs)"},
         "gpu_launches": launches,
         "clocks": clocks,
         "kernels": kernels,
@@ -541,6 +544,88 @@ def adjoint_extra(n=128, steps=100, every=10, viscosity=0.01):
             "timing": "CUDA events; adjoint = first forward pass + segment recomputation + reverse steps"}
 
 
+def adjoint_long(n=512, steps=400, check_n=256, viscosity=NU, snapshots=0):
+    """The long-horizon adjoint workload: Taylor-Green at Re 1600 on n^3 plus
+    the seeded solenoidal perturbation (seed 1; |k| <= 4, RMS 1e-2,
+    projected), `steps` steps at CFL 0.5, loss 1/2 |u(T) - u_target|^2 with the
+    target from the seed-2 forward run; mixed-precision forward and adjoint
+    with the binomial checkpoint schedule sized to the device memory.  Reports
+    forward steps/s, the adjoint/forward device-time ratio, the snapshots and
+    the device memory in use; then, on check_n^3 over the same final time,
+    the mixed-precision gradient against the FP64 adjoint gradient."""
+    import numpy as np
+    import psutil
+    import solver_b200 as sb
+    from solver_b200.adjoint import perturbed_taylor_green, upload_initial
+
+    # the host side holds about 30 padded fields at the largest size
+    need = 30 * 8 * (n + 3) ** 3
+    avail = psutil.virtual_memory().available
+    if avail < 2 * need:
+        raise RuntimeError(f"adjoint_long: {avail / 1e9:.0f} GB of host memory available, "
+                           f"{2 * need / 1e9:.0f} GB wanted")
+
+    def case(size, nsteps, precision):
+        h = 2.0 * math.pi / size
+        ctx = sb.Context(sb.Grid(size, size, size, h, h, h), [sb.PERIODIC] * 6, precision=precision)
+        dt = tg_dt(size)
+        prm = sb.step_params(viscosity, dt, MAX_IT, TOL)
+        state = perturbed_taylor_green(ctx, viscosity, dt, seed=1)
+        other = perturbed_taylor_green(ctx, viscosity, dt, seed=2)
+        upload_initial(ctx, other)
+        t0 = time.perf_counter()
+        ctx.run_steps(prm, nsteps)
+        target_s = time.perf_counter() - t0
+        tst = ctx.download_state()
+        target = [tst[c] for c in "uvw"]
+        del tst, other
+        return ctx, prm, state, target, target_s
+
+    ctx, prm, state, target, target_s = case(n, steps, sb.OF_MIXED)
+    upload_initial(ctx, state)
+    del state
+    _, info = ctx.adjoint_gradient_binomial(prm, steps, target, snapshots=snapshots)
+    ctx_bytes = ctx.device_bytes()
+    ctx.close()
+    del target
+    fwd_ms = info["forward_ms"]
+    total_ms = info["forward_ms"] + info["backward_ms"]
+    check_steps = steps * check_n // n
+    ctx, prm, state, target, _ = case(check_n, check_steps, sb.OF_FP64)
+    upload_initial(ctx, state)
+    g64, i64 = ctx.adjoint_gradient_binomial(prm, check_steps, target)
+    ctx.set_precision(sb.OF_MIXED)
+    upload_initial(ctx, state)
+    g32, i32 = ctx.adjoint_gradient_binomial(prm, check_steps, target)
+    ctx.close()
+    gmax = max(float(np.max(np.abs(a))) for a in g64)
+    gerr = max(float(np.max(np.abs(a - b))) for a, b in zip(g32, g64)) / gmax
+    return {
+        "metric": f"adjoint/forward time ratio, Taylor-Green {n}^3 Re 1600, {steps} steps, mixed",
+        "value": total_ms / fwd_ms, "unit": "x", "higher_is_better": False, "n_gpus": 1,
+        "dtype": "f64+f32", "data": "synthetic (Taylor-Green + seeded solenoidal perturbation)",
+        "config": {"workload": f"taylor_green_3d_{n}_adjoint", "n": n, "steps": steps,
+                   "viscosity": viscosity, "dt": prm.dt, "poisson_tolerance": TOL,
+                   "perturbation": "seed 1, |k| <= 4, RMS 1e-2; target: seed 2 forward run",
+                   "schedule": "binomial (optimal revolve), snapshots sized to device memory"},
+        "forward_steps_per_s": steps / (fwd_ms / 1000.0),
+        "forward_ms": fwd_ms, "adjoint_total_ms": total_ms,
+        "target_run_wall_s": target_s,
+        "snapshots": info["snapshots"], "forward_steps_run": info["forward_steps"],
+        "loss": info["loss"], "grad_viscosity": info["grad_viscosity"],
+        "device_bytes_context": ctx_bytes, "device_bytes_adjoint": info["device_bytes"],
+        "device_bytes_in_use": info["device_bytes_in_use"],
+        "check": {"n": check_n, "steps": check_steps,
+                  "mixed_vs_fp64_gradient_rel_maxnorm": gerr,
+                  "mixed_vs_fp64_grad_viscosity_rel": abs(i32["grad_viscosity"] - i64["grad_viscosity"])
+                  / abs(i64["grad_viscosity"]),
+                  "fp64_snapshots": i64["snapshots"], "fp64_forward_steps_run": i64["forward_steps"],
+                  "fp64_ratio": (i64["forward_ms"] + i64["backward_ms"]) / i64["forward_ms"]},
+        "timing": "CUDA events inside the adjoint call: forward = its first pass over the steps "
+                  "(plain steps plus snapshot copies); total = that pass + recomputation + reverse steps",
+    }
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__)
     ap.add_argument("--gpus", type=int, default=1)
@@ -555,7 +640,13 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the mixed-precision and adjoint measurements of the FP64 1-GPU line")
+    ap.add_argument("--adjoint-long", action="store_true",
+                    help="run the long-horizon adjoint workload (512^3, 400 steps, mixed; "
+                         "minutes of GPU time) instead of the step benchmark")
     args = ap.parse_args()
+    if args.adjoint_long:
+        print(json.dumps(adjoint_long()), flush=True)
+        return 0
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")
     if args.cpu_sample_n is None:

@@ -247,6 +247,18 @@ of_status of_sample_line(of_ctx* ctx, int field, int axis, int i, int j, int k, 
 of_status of_run_steps(of_ctx* ctx, const of_step_params* params, int steps,
                        of_step_metrics* metrics);
 
+/* One step of a host-resident state: of_state_upload of the arrays,
+ * of_run_steps(1) and of_state_download back into the same arrays, with
+ * has_previous_advection and metrics in/out -- the call a caller that keeps
+ * its TaylorGreenState / LidDrivenCavityState on the host makes per step
+ * (run_taylor_green_steps with step_count 1).  When the three adv_* arrays
+ * are pinned (cudaHostAlloc / cudaHostRegister), the new AB2 history is copied
+ * back while the pressure solve runs.  On failure the arrays hold the state
+ * they were called with. */
+of_status of_step_host(of_ctx* ctx, const of_step_params* params, double* u, double* v, double* w,
+                       double* adv_u, double* adv_v, double* adv_w, double* p_total,
+                       int* has_previous_advection, of_step_metrics* metrics);
+
 /* ---- tangent-linear and adjoint runs -------------------------------------- */
 
 /* No counterpart in the reference: the discrete derivatives of of_run_steps
@@ -263,6 +275,8 @@ typedef struct {
   double forward_ms;       /* device time of the first forward pass */
   double backward_ms;      /* device time of the recomputation and reverse steps */
   size_t device_bytes;     /* device memory held by the tangent-linear / adjoint buffers */
+  int snapshots;           /* saved states besides the initial one */
+  size_t device_bytes_in_use; /* device memory in use after the forward pass (all allocations) */
 } of_adjoint_info;
 
 /* du, dv, dw (host, padded): a perturbation of the active entries of the
@@ -282,6 +296,31 @@ of_status of_adjoint_gradient(of_ctx* ctx, const of_step_params* params, int ste
                               int checkpoint_every, const double* target_u,
                               const double* target_v, const double* target_w, double* grad_u,
                               double* grad_v, double* grad_w, of_adjoint_info* info);
+
+/* The same gradient with the optimal binomial checkpoint schedule ("revolve",
+ * Griewank & Walther, ACM TOMS 26, 2000): `snapshots` saved states besides the
+ * initial one, placed so that the number of recomputed forward steps is the
+ * least possible; snapshots = 0 takes as many as fit in the free device memory
+ * (2 GiB kept free, at most 64).  The work set is leaner than
+ * of_adjoint_gradient's (no tangent-linear buffers; the working state shares
+ * the context's scratch), which is what lets 512^3 runs of hundreds of steps
+ * fit one device.  steps <= 4096.  Every reverse step sees the same
+ * recomputed state as in of_adjoint_gradient, so the results agree to
+ * rounding (the transposed advection accumulates with atomics). */
+of_status of_adjoint_gradient_binomial(of_ctx* ctx, const of_step_params* params, int steps,
+                                       int snapshots, const double* target_u,
+                                       const double* target_v, const double* target_w,
+                                       double* grad_u, double* grad_v, double* grad_w,
+                                       of_adjoint_info* info);
+
+/* Host-only: forward steps the binomial schedule recomputes to reverse
+ * `steps` steps with `snapshots` free snapshots -- from a saved initial state
+ * alone (reverse_cost; Griewank's closed form for snapshots + 1 checkpoints)
+ * and right after the forward pass that placed the first snapshots
+ * (after_forward_cost, what of_adjoint_gradient_binomial runs beyond its
+ * forward pass).  Either pointer may be NULL. */
+of_status of_adjoint_schedule_cost(int steps, int snapshots, long long* reverse_cost,
+                                   long long* after_forward_cost);
 
 /* ---- allocation-free entry point ---------------------------------------- */
 

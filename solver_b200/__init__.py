@@ -242,6 +242,24 @@ class Context:
     def tg_init(self, viscosity, dt, mode=0):
         _capi.check(self._lib.of_tg_init(self._h, float(viscosity), float(dt), int(mode)))
 
+    def step_host(self, params: _capi.OfStepParams, state):
+        """One step of a host-resident state (dict of u, v, w, adv_u, adv_v,
+        adv_w, p arrays, has_previous_advection, metrics), updated in place:
+        upload, step and download in one call; pinned adv_* arrays get the new
+        AB2 history while the pressure solve runs.  Returns the metrics."""
+        names = ("u", "v", "w", "adv_u", "adv_v", "adv_w", "p")
+        for name, loc in zip(names, "uvwuvwp"):
+            _check_shape(self.grid, state[name], loc, "step_host")
+        hp = C.c_int(int(bool(state.get("has_previous_advection", 0))))
+        m = _capi.OfStepMetrics()
+        for k, val in (state.get("metrics") or {}).items():
+            setattr(m, k, val)
+        _capi.check(self._lib.of_step_host(self._h, C.byref(params), *(_dp(state[k]) for k in names),
+                                           C.byref(hp), C.byref(m)))
+        state["has_previous_advection"] = hp.value
+        state["metrics"] = _struct_dict(m)
+        return state["metrics"]
+
     def run_steps(self, params: _capi.OfStepParams, steps: int):
         m = _capi.OfStepMetrics()
         _capi.check(self._lib.of_run_steps(self._h, C.byref(params), int(steps), C.byref(m)))
@@ -275,6 +293,29 @@ class Context:
                                                   int(checkpoint_every), *map(_dp, target),
                                                   *map(_dp, grad), C.byref(info)))
         return grad, _struct_dict(info)
+
+    def adjoint_gradient_binomial(self, params: _capi.OfStepParams, steps: int, target,
+                                  snapshots: int = 0):
+        """adjoint_gradient with the optimal binomial checkpoint schedule and
+        `snapshots` saved states (0: as many as fit in device memory)."""
+        g = self.grid
+        for a, loc in zip(target, "uvw"):
+            _check_shape(g, a, loc, "adjoint_gradient_binomial")
+        grad = [g.zeros(c) for c in "uvw"]
+        info = _capi.OfAdjointInfo()
+        _capi.check(self._lib.of_adjoint_gradient_binomial(
+            self._h, C.byref(params), int(steps), int(snapshots), *map(_dp, target),
+            *map(_dp, grad), C.byref(info)))
+        return grad, _struct_dict(info)
+
+
+def adjoint_schedule_cost(steps: int, snapshots: int):
+    """(reverse_cost, after_forward_cost): forward steps the binomial schedule
+    recomputes for `steps` steps and `snapshots` free snapshots (host only)."""
+    a, b = C.c_longlong(), C.c_longlong()
+    _capi.check(_capi.load().of_adjoint_schedule_cost(int(steps), int(snapshots), C.byref(a),
+                                                      C.byref(b)))
+    return a.value, b.value
 
 
 def step_params(viscosity, dt, max_iterations, tolerance, variant=OF_CORRECTION_TAYLOR_GREEN,

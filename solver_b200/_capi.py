@@ -23,7 +23,8 @@ EXPORTED_SYMBOLS = (
     "of_solve_pressure_poisson", "of_project_velocity", "of_state_upload", "of_state_download",
     "of_tg_init", "of_run_steps", "of_stream", "of_kernel_class_count", "of_kernel_class_name",
     "of_profile_enable", "of_profile_reset", "of_profile_read", "of_tangent_linear",
-    "of_adjoint_gradient", "of_pressure_rhs_noalloc",
+    "of_adjoint_gradient", "of_pressure_rhs_noalloc", "of_step_host",
+    "of_adjoint_gradient_binomial", "of_adjoint_schedule_cost",
 )
 
 
@@ -81,7 +82,8 @@ class OfStepParams(C.Structure):
 class OfAdjointInfo(C.Structure):
     _fields_ = [("loss", C.c_double), ("grad_viscosity", C.c_double), ("forward_steps", C.c_int),
                 ("forward_ms", C.c_double), ("backward_ms", C.c_double),
-                ("device_bytes", C.c_size_t)]
+                ("device_bytes", C.c_size_t), ("snapshots", C.c_int),
+                ("device_bytes_in_use", C.c_size_t)]
 
 
 DP = C.POINTER(C.c_double)
@@ -115,6 +117,8 @@ def load():
         lib.of_tg_init.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int]
         lib.of_run_steps.argtypes = [C.c_void_p, C.POINTER(OfStepParams), C.c_int,
                                      C.POINTER(OfStepMetrics)]
+        lib.of_step_host.argtypes = [C.c_void_p, C.POINTER(OfStepParams)] + [DP] * 7 + \
+            [C.POINTER(C.c_int), C.POINTER(OfStepMetrics)]
         lib.of_stream.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
         # device pointers (u, v, w, pressure_rhs, stream) as c_void_p
         lib.of_pressure_rhs_noalloc.argtypes = [C.POINTER(OfGrid), C.c_double, C.c_double] + \
@@ -122,6 +126,9 @@ def load():
         lib.of_tangent_linear.argtypes = [C.c_void_p, C.POINTER(OfStepParams), C.c_int] + [DP] * 6
         lib.of_adjoint_gradient.argtypes = [C.c_void_p, C.POINTER(OfStepParams), C.c_int,
                                             C.c_int] + [DP] * 6 + [C.POINTER(OfAdjointInfo)]
+        lib.of_adjoint_gradient_binomial.argtypes = lib.of_adjoint_gradient.argtypes
+        lib.of_adjoint_schedule_cost.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_longlong),
+                                                 C.POINTER(C.c_longlong)]
         lib.of_kernel_class_name.restype = C.c_char_p
         lib.of_profile_enable.argtypes = [C.c_int]
         lib.of_profile_read.argtypes = [C.c_int, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),

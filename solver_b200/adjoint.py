@@ -35,39 +35,45 @@ def unique_loss(vel, target):
                      for c, n in enumerate("uvw"))
 
 
-def _face_coords(grid: Grid, loc):
-    """Coordinates of the storage points of a padded field (active and ghost)."""
+def _axis_coords(grid: Grid, loc):
+    """1-D storage coordinates (x, y, z) of a padded field, ghosts included."""
     shape = grid.shape(loc)
-    axes = []
-    for axis, (n, h, name) in enumerate(zip((grid.nx, grid.ny, grid.nz), (grid.dx, grid.dy, grid.dz),
-                                             "xyz")):
-        size = shape[2 - axis]
-        idx = np.arange(size) - 1.0
-        face = (loc == "u" and name == "x") or (loc == "v" and name == "y") or (loc == "w" and name == "z")
-        axes.append(idx * h if face else (idx + 0.5) * h)
-    zz, yy, xx = np.meshgrid(axes[2], axes[1], axes[0], indexing="ij")
-    return xx, yy, zz
+    out = []
+    for axis, (h, name) in enumerate(zip((grid.dx, grid.dy, grid.dz), "xyz")):
+        idx = np.arange(shape[2 - axis]) - 1.0
+        face = (loc, name) in (("u", "x"), ("v", "y"), ("w", "z"))
+        out.append(idx * h if face else (idx + 0.5) * h)
+    return out
 
 
 def smooth_field(grid: Grid, seed, rms=1.0, kmax=4):
     """Velocity-shaped random field: Fourier modes 0 < |k| <= kmax with
-    standard-normal cosine and sine amplitudes from numpy's Generator(seed),
-    scaled to the given RMS over the active entries (padded arrays, edges and
-    corners zero)."""
+    standard-normal cosine and sine amplitudes from numpy's Generator(seed)
+    (drawn per component, modes in (kx, ky, kz) lexicographic order), scaled
+    to the given RMS over the active entries (padded arrays, edges and corners
+    zero).  a cos(k.x) + b sin(k.x) = Re((a - ib) e^{ik.x}) is summed axis by
+    axis, so a 512^3 field costs three small contractions and one matrix
+    product instead of a pass over the grid per mode."""
     g = grid
     rng = np.random.default_rng(seed)
-    modes = [(kx, ky, kz) for kx in range(-kmax, kmax + 1) for ky in range(-kmax, kmax + 1)
-             for kz in range(-kmax, kmax + 1)
+    ks = np.arange(-kmax, kmax + 1)
+    modes = [(kx, ky, kz) for kx in ks for ky in ks for kz in ks
              if 0 < kx * kx + ky * ky + kz * kz <= kmax * kmax and (g.nz > 1 or kz == 0)]
     out = []
     for comp in "uvw":
-        xx, yy, zz = _face_coords(g, comp)
         f = np.zeros(g.shape(comp))
         if not (comp == "w" and g.nz == 1):
+            coef = np.zeros((ks.size, ks.size, ks.size), dtype=np.complex128)  # [kz, ky, kx]
             for (kx, ky, kz) in modes:
                 a, b = rng.standard_normal(2)
-                ph = kx * xx + ky * yy + kz * zz
-                f += a * np.cos(ph) + b * np.sin(ph)
+                coef[kz + kmax, ky + kmax, kx + kmax] += a - 1j * b
+            x, y, z = _axis_coords(g, comp)
+            ex = np.exp(1j * np.outer(ks, x))  # [kx, i]
+            ey = np.exp(1j * np.outer(ks, y))  # [ky, j]
+            ez = np.exp(1j * np.outer(ks, z))  # [kz, k]
+            t = np.einsum("abc,ci->abi", coef, ex)  # [kz, ky, i]
+            t = np.einsum("bj,abi->aji", ey, t).reshape(ks.size, -1)  # [kz, j*i]
+            f = (ez.real.T @ t.real - ez.imag.T @ t.imag).reshape(g.shape(comp))
         out.append(f)
     cur_rms = math.sqrt(sum(float(np.mean(a[1:-1, 1:-1, 1:-1] ** 2)) for a in out) / 3.0)
     for a in out:

@@ -76,21 +76,28 @@ struct SavedState {
   bool clean = false;
 };
 
+// What a work set serves: the tangent-linear run, the adjoint with a
+// checkpoint every `every` steps, or the adjoint with a binomial schedule
+// (lean: no tangent buffers, the working state and the recomputed
+// intermediates share the context's scratch, `slots` saved states).
+enum AdjKind { kAdjTangent = 0, kAdjSegments = 1, kAdjBinomial = 2 };
+
 struct AdjWork {
   std::vector<double*> owned;
   size_t bytes = 0;
-  int steps = 0, every = 0;
+  int steps = 0, every = 0, kind = -1, snapshots = 0;
   // tangent-linear state and the base velocity it is linearised about
-  double *t_vel[3], *t_adv_prev[3], *t_adv_cur[3], *t_corr[3], *t_p, *base_cur[3];
+  double *t_vel[3] = {}, *t_adv_prev[3] = {}, *t_adv_cur[3] = {}, *t_corr[3] = {}, *t_p = nullptr,
+         *base_cur[3] = {};
   // adjoint variables
-  double *lam_vel[3], *lam_corr[3], *lam_pred[3], *lam_b[3], *lam_cur[3], *lam_prev[3],
-      *lam_advtot[3], *target[3], *out[3];
-  double *lam_p, *lam_phi, *lam_q;
+  double *lam_vel[3] = {}, *lam_corr[3] = {}, *lam_pred[3] = {}, *lam_b[3] = {}, *lam_cur[3] = {},
+         *lam_prev[3] = {}, *lam_advtot[3] = {}, *target[3] = {}, *out[3] = {};
+  double *lam_p = nullptr, *lam_phi = nullptr, *lam_q = nullptr;
   // recomputed intermediates of the step being differentiated
-  double *y[3][3], *rc_adv[3], *rc_corr[3];
-  // working state of a segment recomputation
-  double *w_vel[3], *w_adv_prev[3], *w_adv_cur[3], *w_corr[3], *w_p;
-  std::vector<SavedState> ckpt, seg;
+  double *y[3][3] = {}, *rc_adv[3] = {}, *rc_corr[3] = {};
+  // working state of a recomputation
+  double *w_vel[3] = {}, *w_adv_prev[3] = {}, *w_adv_cur[3] = {}, *w_corr[3] = {}, *w_p = nullptr;
+  std::vector<SavedState> ckpt, seg, slots;
   std::vector<double*> phi;  // per step: compact pressure correction + its shift (may be empty)
   double* acc = nullptr;  // [0] loss, [1] d/dnu (direct), [2] sum mu.D y of the sweeps
   ~AdjWork() {
@@ -133,6 +140,8 @@ struct of_ctx {
   double* prhs = nullptr;       // padded pressure rhs
   double* phi = nullptr;        // padded pressure correction (operator API)
   double* diag = nullptr;       // diagnostics reductions (4 doubles)
+  cudaStream_t side = nullptr;  // of_step_host: download of the AB2 history
+  cudaEvent_t adv_ready = nullptr;
 
   ofb::RedBuf rb{};
   ofb::SolveScalars* sc = nullptr;       // device
@@ -168,6 +177,11 @@ struct of_ctx {
     if(sc_host) cudaFreeHost(sc_host);
     ofb::poisson_plan_destroy(poisson);
     ofb::adi_plan_destroy(adi);
+    if(side) {
+      cudaStreamSynchronize(side);
+      cudaStreamDestroy(side);
+    }
+    if(adv_ready) cudaEventDestroy(adv_ready);
     if(stream) cudaStreamDestroy(stream);
   }
 
@@ -387,6 +401,12 @@ struct StepHooks {
   // (a recomputed step then reproduces the original bit for bit)
   double* phi_store = nullptr;
   const double* phi_load = nullptr;
+  // when set, this step's advection term (the next step's AB2 history) is
+  // copied to these host arrays on `side` as soon as the predictor has
+  // formed it, overlapping the rest of the step
+  double* const* adv_host = nullptr;
+  cudaStream_t side = nullptr;
+  cudaEvent_t adv_ready = nullptr;
 };
 
 // One projection step on `st` (the loop body of run_taylor_green_steps,
@@ -427,6 +447,13 @@ ofb::SolveScalars forward_step(of_ctx* ctx, const of_step_params* prm, const std
     ofb::launch_predictor_rest(pa, s);
   } else {
     ofb::launch_predictor_rhs(pa, s);
+  }
+  if(hk != nullptr && hk->adv_host != nullptr) {
+    OFB_CHECK(cudaEventRecord(hk->adv_ready, s));
+    OFB_CHECK(cudaStreamWaitEvent(hk->side, hk->adv_ready, 0));
+    for(int c = 0; c < 3; ++c)
+      OFB_CHECK(cudaMemcpyAsync(hk->adv_host[c], st.adv_cur[c], ctx->size(1 + c) * sizeof(double),
+                                cudaMemcpyDeviceToHost, hk->side));
   }
   // solve_predictor_adi
   double* pred[3];
@@ -499,55 +526,97 @@ ofb::SolveScalars forward_step(of_ctx* ctx, const of_step_params* prm, const std
 
 size_t g_cells(of_ctx* ctx) { return static_cast<size_t>(ctx->g.nx) * ctx->g.ny * ctx->g.nz; }
 
-AdjWork* adj_work(of_ctx* ctx, int steps, int every) {
+SavedState alloc_saved(of_ctx* ctx, AdjWork* W) {
+  SavedState t;
+  for(int c = 0; c < 3; ++c) {
+    t.vel[c] = W->alloc(ctx->size(1 + c), ctx->stream);
+    t.adv_prev[c] = W->alloc(ctx->size(1 + c), ctx->stream);
+  }
+  t.p = W->alloc(ctx->size(0), ctx->stream);
+  return t;
+}
+
+size_t saved_bytes(of_ctx* ctx) {
+  return sizeof(double) * (ctx->size(0) + 2 * (ctx->size(1) + ctx->size(2) + ctx->size(3)));
+}
+
+// Keeps every step's pressure-solve result when it fits comfortably (under
+// 40% of the free device memory): recomputed steps then skip their pressure
+// solves.
+void keep_pressure_results(of_ctx* ctx, AdjWork* W, int steps) {
+  size_t free_b = 0, total_b = 0;
+  OFB_CHECK(cudaMemGetInfo(&free_b, &total_b));
+  const size_t per = (static_cast<size_t>(g_cells(ctx)) + 1) * sizeof(double);
+  if(static_cast<double>(per) * steps < 0.4 * static_cast<double>(free_b))
+    for(int n = 0; n < steps; ++n) W->phi.push_back(W->alloc(per / sizeof(double), ctx->stream));
+}
+
+constexpr int kMaxSnapshots = 64;
+constexpr size_t kSnapshotReserve = size_t(2) << 30;  // device memory left free by the auto sizing
+
+// Work set of a tangent-linear or adjoint run; kept on the context while the
+// same kind of run repeats.  `every`: checkpoint interval (kAdjSegments);
+// `snapshots`: saved states besides the initial one (kAdjBinomial; 0 sizes
+// them to the free device memory).
+AdjWork* adj_work(of_ctx* ctx, int kind, int steps, int every, int snapshots = 0) {
   AdjWork* W = ctx->adj;
-  const int nseg = (steps + every - 1) / every;
-  if(W != nullptr && W->steps == steps && W->every == every) return W;
+  if(W != nullptr && W->kind == kind && W->steps == steps && W->every == every &&
+     (kind != kAdjBinomial || snapshots == 0 || W->snapshots == std::min(snapshots, steps - 1)))
+    return W;
   ctx->sync();
   delete W;
   ctx->adj = nullptr;
   W = new AdjWork();
+  ctx->adj = W;  // owned by the context from here, so a failed allocation frees it
   cudaStream_t s = ctx->stream;
   auto face = [&](int c) { return ctx->size(1 + c); };
   const size_t cell = ctx->size(0);
   for(int c = 0; c < 3; ++c) {
-    for(double** b : {&W->t_vel[c], &W->t_adv_prev[c], &W->t_adv_cur[c], &W->t_corr[c], &W->base_cur[c],
-                      &W->lam_vel[c], &W->lam_corr[c], &W->lam_pred[c], &W->lam_b[c], &W->lam_cur[c],
-                      &W->lam_prev[c], &W->lam_advtot[c], &W->target[c], &W->out[c], &W->rc_adv[c],
-                      &W->rc_corr[c], &W->w_vel[c], &W->w_adv_prev[c], &W->w_adv_cur[c], &W->w_corr[c]})
+    for(double** b : {&W->lam_vel[c], &W->lam_corr[c], &W->lam_pred[c], &W->lam_b[c], &W->lam_cur[c],
+                      &W->lam_prev[c], &W->lam_advtot[c], &W->w_vel[c], &W->w_adv_prev[c]})
       *b = W->alloc(face(c), s);
     for(int a = 0; a < 3; ++a) W->y[c][a] = W->alloc(face(c), s);
+    if(kind == kAdjBinomial) {
+      // the target is read once, into lam_corr, before the reverse steps use
+      // it; the gradient is assembled in lam_b after the last of them
+      W->target[c] = W->lam_corr[c];
+      W->out[c] = W->lam_b[c];
+      continue;
+    }
+    for(double** b : {&W->target[c], &W->out[c], &W->rc_adv[c], &W->rc_corr[c], &W->w_adv_cur[c],
+                      &W->w_corr[c]})
+      *b = W->alloc(face(c), s);
+    if(kind == kAdjTangent)
+      for(double** b : {&W->t_vel[c], &W->t_adv_prev[c], &W->t_adv_cur[c], &W->t_corr[c], &W->base_cur[c]})
+        *b = W->alloc(face(c), s);
   }
-  W->t_p = W->alloc(cell, s);
+  if(kind == kAdjTangent) W->t_p = W->alloc(cell, s);
   W->w_p = W->alloc(cell, s);
   W->lam_p = W->alloc(cell, s);
   W->lam_phi = W->alloc(cell, s);
   W->lam_q = W->alloc(cell, s);
   W->acc = W->alloc(4, s);
-  auto saved = [&]() {
-    SavedState t;
-    for(int c = 0; c < 3; ++c) {
-      t.vel[c] = W->alloc(face(c), s);
-      t.adv_prev[c] = W->alloc(face(c), s);
+  if(kind == kAdjSegments) {
+    const int nseg = (steps + every - 1) / every;
+    for(int k = 0; k < nseg; ++k) W->ckpt.push_back(alloc_saved(ctx, W));
+    for(int k = 0; k < every && k < steps; ++k) W->seg.push_back(alloc_saved(ctx, W));
+    if(every > 1) keep_pressure_results(ctx, W, steps);
+  } else if(kind == kAdjBinomial) {
+    W->slots.push_back(alloc_saved(ctx, W));  // the initial state
+    if(steps > 1) keep_pressure_results(ctx, W, steps);
+    int want = std::min(steps - 1, snapshots > 0 ? snapshots : kMaxSnapshots);
+    if(snapshots == 0) {
+      size_t free_b = 0, total_b = 0;
+      OFB_CHECK(cudaMemGetInfo(&free_b, &total_b));
+      const size_t room = free_b > kSnapshotReserve ? (free_b - kSnapshotReserve) / saved_bytes(ctx) : 0;
+      want = std::min<long long>(want, static_cast<long long>(room));
     }
-    t.p = W->alloc(cell, s);
-    return t;
-  };
-  for(int k = 0; k < nseg; ++k) W->ckpt.push_back(saved());
-  for(int k = 0; k < every && k < steps; ++k) W->seg.push_back(saved());
-  // Keep every step's pressure-solve result when it fits comfortably (under
-  // 40% of the free device memory): the recomputation of a segment then skips
-  // its pressure solves.
-  if(every > 1) {
-    size_t free_b = 0, total_b = 0;
-    OFB_CHECK(cudaMemGetInfo(&free_b, &total_b));
-    const size_t per = (static_cast<size_t>(g_cells(ctx)) + 1) * sizeof(double);
-    if(static_cast<double>(per) * steps < 0.4 * static_cast<double>(free_b))
-      for(int n = 0; n < steps; ++n) W->phi.push_back(W->alloc(per / sizeof(double), s));
+    for(int k = 0; k < want; ++k) W->slots.push_back(alloc_saved(ctx, W));
+    W->snapshots = want;
   }
+  W->kind = kind;
   W->steps = steps;
   W->every = every;
-  ctx->adj = W;
   return W;
 }
 
@@ -557,7 +626,7 @@ AdjWork* adj_work(of_ctx* ctx, int steps, int every) {
 void adopt_edges(of_ctx* ctx, AdjWork* W) {
   for(int c = 0; c < 3; ++c)
     for(double* b : {W->w_vel[c], W->w_corr[c], W->rc_corr[c], W->base_cur[c]})
-      ctx->d2d(b, ctx->vel[c], 1 + c);
+      if(b != nullptr) ctx->d2d(b, ctx->vel[c], 1 + c);
 }
 
 void save_state(of_ctx* ctx, const StepState& st, SavedState& out) {
@@ -969,7 +1038,7 @@ of_status of_state_upload(of_ctx* ctx, const double* u, const double* v, const d
       require_ptr(ain[c], "previous advection");
       ctx->upload(ctx->vel[c], vin[c], 1 + c);
       ctx->upload(ctx->adv_prev[c], ain[c], 1 + c);
-      ctx->upload(ctx->adv_cur[c], ain[c], 1 + c);
+      ctx->d2d(ctx->adv_cur[c], ctx->adv_prev[c], 1 + c);
       // Edge and corner ghosts are never written by any kernel; every
       // velocity-shaped buffer carries the state's so that full-copy
       // semantics of the reference hold without per-step copies.
@@ -1112,42 +1181,111 @@ of_status of_sample_line(of_ctx* ctx, int field, int axis, int i, int j, int k, 
   });
 }
 
+namespace {
+
+// Parameter checks of run_*_steps (the messages of the reference's callees).
+void check_step_params(const of_step_params* prm, int steps) {
+  require_ptr(prm, "step parameters");
+  if(steps < 0) fail(OF_INVALID_ARGUMENT, "run_taylor_green_steps expects a non-negative step count");
+  if(prm->dt <= 0.0) fail(OF_INVALID_ARGUMENT, "build_pressure_rhs expects dt > 0");
+  if(prm->density <= 0.0) fail(OF_INVALID_ARGUMENT, "build_pressure_rhs expects density > 0");
+  if(prm->poisson_max_iterations <= 0)
+    fail(OF_INVALID_ARGUMENT, "solve_pressure_poisson expects iterations > 0");
+  if(prm->poisson_tolerance <= 0.0)
+    fail(OF_INVALID_ARGUMENT, "solve_pressure_poisson expects tolerance > 0");
+}
+
+// One step of the resident state and its metrics update; on failure the
+// state stays at the last completed step.
+void resident_step(of_ctx* ctx, const of_step_params* prm, const std::string& name, const StepHooks* hk) {
+  StepState st = resident_state(ctx);
+  ofb::SolveScalars d;
+  try {
+    d = forward_step(ctx, prm, name, ctx->metrics.step + 1, st, hk);
+  } catch(...) {
+    set_resident_state(ctx, st);
+    throw;
+  }
+  set_resident_state(ctx, st);
+  of_step_metrics& m = ctx->metrics;
+  m.step += 1;
+  m.time += prm->dt;
+  m.dt = prm->dt;
+  m.max_cfl = d.max_cfl;
+  m.max_velocity_change = d.max_dv;
+  m.divergence_l2 = d.div_after_l2;
+  if(prm->track_max_divergence)
+    m.max_divergence_l2 = m.max_divergence_l2 < d.div_after_l2 ? d.div_after_l2 : m.max_divergence_l2;
+  m.pressure_iterations = d.iterations;
+  m.pressure_relative_residual = d.rel;
+}
+
+bool pinned_host(const void* p) {
+  cudaPointerAttributes a{};
+  if(cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+}  // namespace
+
 of_status of_run_steps(of_ctx* ctx, const of_step_params* prm, int steps, of_step_metrics* out) {
   return guarded([&] {
     require_ctx(ctx);
-    require_ptr(prm, "step parameters");
-    if(steps < 0) fail(OF_INVALID_ARGUMENT, "run_taylor_green_steps expects a non-negative step count");
-    if(prm->dt <= 0.0) fail(OF_INVALID_ARGUMENT, "build_pressure_rhs expects dt > 0");
-    if(prm->density <= 0.0) fail(OF_INVALID_ARGUMENT, "build_pressure_rhs expects density > 0");
-    if(prm->poisson_max_iterations <= 0)
-      fail(OF_INVALID_ARGUMENT, "solve_pressure_poisson expects iterations > 0");
-    if(prm->poisson_tolerance <= 0.0)
-      fail(OF_INVALID_ARGUMENT, "solve_pressure_poisson expects tolerance > 0");
+    check_step_params(prm, steps);
     const std::string name = prm->solver_name ? prm->solver_name : "Taylor-Green";
-    const double dt = prm->dt;
-    for(int step = 0; step < steps; ++step) {
-      StepState st = resident_state(ctx);
-      ofb::SolveScalars d;
-      try {
-        d = forward_step(ctx, prm, name, ctx->metrics.step + 1, st);
-      } catch(...) {
-        set_resident_state(ctx, st);
-        throw;
-      }
-      set_resident_state(ctx, st);
-      of_step_metrics& m = ctx->metrics;
-      m.step += 1;
-      m.time += dt;
-      m.dt = dt;
-      m.max_cfl = d.max_cfl;
-      m.max_velocity_change = d.max_dv;
-      m.divergence_l2 = d.div_after_l2;
-      if(prm->track_max_divergence)
-        m.max_divergence_l2 = m.max_divergence_l2 < d.div_after_l2 ? d.div_after_l2 : m.max_divergence_l2;
-      m.pressure_iterations = d.iterations;
-      m.pressure_relative_residual = d.rel;
-    }
+    for(int step = 0; step < steps; ++step) resident_step(ctx, prm, name, nullptr);
     if(out) *out = ctx->metrics;
+  });
+}
+
+of_status of_step_host(of_ctx* ctx, const of_step_params* prm, double* u, double* v, double* w,
+                       double* adv_u, double* adv_v, double* adv_w, double* p_total,
+                       int* has_previous_advection, of_step_metrics* metrics) {
+  return guarded([&] {
+    require_ctx(ctx);
+    require_ptr(has_previous_advection, "has_previous_advection");
+    check_step_params(prm, 1);
+    const of_status up = of_state_upload(ctx, u, v, w, adv_u, adv_v, adv_w, p_total, *has_previous_advection,
+                                         metrics);
+    if(up != OF_OK) fail(up, of_last_error());
+    const std::string name = prm->solver_name ? prm->solver_name : "Taylor-Green";
+    double* adv[3] = {adv_u, adv_v, adv_w};
+    StepHooks hk;
+    const bool overlap = pinned_host(adv_u) && pinned_host(adv_v) && pinned_host(adv_w);
+    if(overlap) {
+      if(ctx->side == nullptr) OFB_CHECK(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
+      if(ctx->adv_ready == nullptr) OFB_CHECK(cudaEventCreateWithFlags(&ctx->adv_ready, cudaEventDisableTiming));
+      hk.adv_host = adv;
+      hk.side = ctx->side;
+      hk.adv_ready = ctx->adv_ready;
+    }
+    try {
+      resident_step(ctx, prm, name, overlap ? &hk : nullptr);
+    } catch(...) {
+      // the history copies may have written this failed step's advection:
+      // put the resident (uploaded) history back into the caller's arrays
+      if(overlap) {
+        cudaStreamSynchronize(ctx->side);
+        for(int c = 0; c < 3; ++c)
+          cudaMemcpyAsync(adv[c], ctx->adv_prev[c], ctx->size(1 + c) * sizeof(double),
+                          cudaMemcpyDeviceToHost, ctx->stream);
+        cudaStreamSynchronize(ctx->stream);
+      }
+      throw;
+    }
+    double* vout[3] = {u, v, w};
+    for(int c = 0; c < 3; ++c) {
+      ctx->download(vout[c], ctx->vel[c], 1 + c);
+      if(!overlap) ctx->download(adv[c], ctx->adv_prev[c], 1 + c);
+    }
+    ctx->download(p_total, ctx->p_total, 0);
+    if(overlap) OFB_CHECK(cudaStreamSynchronize(ctx->side));
+    ctx->sync();
+    *has_previous_advection = ctx->has_prev;
+    if(metrics) *metrics = ctx->metrics;
   });
 }
 
@@ -1166,7 +1304,7 @@ of_status of_tangent_linear(of_ctx* ctx, const of_step_params* prm, int steps, c
     if(steps < 1) fail(OF_INVALID_ARGUMENT, "the tangent-linear run needs at least one step");
     require_adjoint_case(ctx, prm);
     const std::string name = prm->solver_name ? prm->solver_name : "Taylor-Green";
-    AdjWork* W = adj_work(ctx, steps, steps);
+    AdjWork* W = adj_work(ctx, kAdjTangent, steps, steps);
     StepState st = resident_state(ctx);
     adopt_edges(ctx, W);
     StepState t{};
@@ -1222,6 +1360,302 @@ of_status of_tangent_linear(of_ctx* ctx, const of_step_params* prm, int steps, c
   });
 }
 
+}  // extern "C"
+
+namespace {
+
+size_t device_in_use() {
+  size_t free_b = 0, total_b = 0;
+  OFB_CHECK(cudaMemGetInfo(&free_b, &total_b));
+  return total_b - free_b;
+}
+
+constexpr int kMaxBinomialSteps = 4096;
+
+// Optimal binomial checkpoint schedule (the "revolve" schedule: Griewank,
+// Optimization Methods and Software 1 (1992); Griewank & Walther, ACM TOMS 26
+// (2000)), by dynamic programming over the n steps still to reverse and the s
+// snapshots still free.  With the state at the start of the n steps saved and
+// the adjoint at their end known, reversing them costs
+//   C(1, s) = 0,   C(n, 0) = n (n - 1) / 2   (advance from the start for each step),
+//   C(n, s) = min over 0 < m < n of  m + C(n - m, s - 1) + C(m, s)
+// forward steps: advance m steps and save, reverse the right part with one
+// snapshot fewer, then the left part with that snapshot free again.  C(n, s)
+// equals the published minimum t n - binom(s + t + 1, t - 1) for s + 1
+// checkpoints, t the smallest with binom(s + t + 1, t) >= n.  D is the same
+// recursion right after the forward pass that reached the end: that pass saved
+// the first split of every level on its way ("spine"), so those advances are
+// free:  D(1, s) = 0,  D(n, 0) = C(n, 0),  D(n, s) = min over m of D(n - m, s - 1) + C(m, s).
+struct Schedule {
+  int n = 0, s = 0;
+  std::vector<long long> C, D;
+  std::vector<int> Cm, Dm;
+  size_t at(int i, int j) const { return static_cast<size_t>(i) * (s + 1) + j; }
+  Schedule(int steps, int snaps) : n(steps), s(snaps) {
+    const size_t size = static_cast<size_t>(n + 1) * (s + 1);
+    C.assign(size, 0);
+    D.assign(size, 0);
+    Cm.assign(size, 0);
+    Dm.assign(size, 0);
+    for(int i = 2; i <= n; ++i) {
+      C[at(i, 0)] = D[at(i, 0)] = static_cast<long long>(i) * (i - 1) / 2;
+      for(int j = 1; j <= s; ++j) {
+        long long best_c = -1, best_d = -1;
+        int m_c = 1, m_d = 1;
+        for(int m = 1; m < i; ++m) {
+          const long long left = C[at(m, j)];
+          const long long c = m + C[at(i - m, j - 1)] + left;
+          const long long d = D[at(i - m, j - 1)] + left;
+          if(best_c < 0 || c < best_c) {
+            best_c = c;
+            m_c = m;
+          }
+          if(best_d < 0 || d < best_d) {
+            best_d = d;
+            m_d = m;
+          }
+        }
+        C[at(i, j)] = best_c;
+        Cm[at(i, j)] = m_c;
+        D[at(i, j)] = best_d;
+        Dm[at(i, j)] = m_d;
+      }
+    }
+  }
+  // the steps before which the forward pass saves the spine snapshots 1, 2, ...
+  std::vector<int> spine() const {
+    std::vector<int> pos;
+    int start = 0, left = n, free = s;
+    while(left > 1 && free > 0) {
+      const int m = Dm[at(left, free)];
+      start += m;
+      left -= m;
+      --free;
+      pos.push_back(start);
+    }
+    return pos;
+  }
+};
+
+// The reverse sweep of a binomial schedule.  The working state `ws` holds the
+// recomputed states; the adjoint step's recomputed intermediates use its
+// scratch halves (AB2 term, corrected velocity), which hold nothing between
+// steps.
+struct BinomialSweep {
+  of_ctx* ctx;
+  const of_step_params* prm;
+  AdjWork* W;
+  const Schedule* sch;
+  std::string name;
+  StepState ws{};
+  int top = 1;
+  long long forward = 0;
+
+  void advance(const SavedState& from, int n0, int k) {
+    load_state(ctx, from, ws);
+    for(int i = 0; i < k; ++i) {
+      StepHooks hk;
+      if(!W->phi.empty()) hk.phi_load = W->phi[n0 + i];
+      forward_step(ctx, prm, name, n0 + i + 1, ws, &hk);
+      ++forward;
+    }
+  }
+  SavedState working() const {
+    SavedState v;
+    for(int c = 0; c < 3; ++c) {
+      v.vel[c] = ws.vel[c];
+      v.adv_prev[c] = ws.adv_prev[c];
+    }
+    v.p = ws.p;
+    v.has_prev = ws.has_prev;
+    v.clean = ws.clean;
+    return v;
+  }
+  void reverse_step(const SavedState& S) {
+    for(int c = 0; c < 3; ++c) {
+      W->rc_adv[c] = ws.adv_cur[c];
+      W->rc_corr[c] = ws.corrected[c];
+    }
+    adjoint_step(ctx, prm, W, S);
+  }
+  // Reverses steps n0 .. n0 + n - 1; the state before step n0 is in
+  // slots[slot], snapshots top .. top + free - 1 are free; on the spine the
+  // state at the split is already in slots[top].
+  void run(int slot, int n0, int n, int free, bool on_spine) {
+    const SavedState& S = W->slots[slot];
+    if(n == 1) {
+      reverse_step(S);
+      return;
+    }
+    if(free == 0) {
+      for(int k = n - 1; k >= 1; --k) {
+        advance(S, n0, k);
+        reverse_step(working());
+      }
+      reverse_step(S);
+      return;
+    }
+    const int m = on_spine ? sch->Dm[sch->at(n, free)] : sch->Cm[sch->at(n, free)];
+    const int mine = top++;
+    if(!on_spine) {
+      advance(S, n0, m);
+      save_state(ctx, ws, W->slots[mine]);
+    }
+    run(mine, n0 + m, n - m, free - 1, on_spine);
+    --top;
+    run(slot, n0, m, free, false);
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+of_status of_adjoint_schedule_cost(int steps, int snapshots, long long* reverse_cost,
+                                   long long* after_forward_cost) {
+  return guarded([&] {
+    if(steps < 1 || steps > kMaxBinomialSteps)
+      fail(OF_INVALID_ARGUMENT, "the binomial schedule supports 1 to 4096 steps");
+    if(snapshots < 0) fail(OF_INVALID_ARGUMENT, "snapshots must be non-negative");
+    const int s = std::min(snapshots, std::max(steps - 1, 0));
+    const Schedule sch(steps, s);
+    if(reverse_cost) *reverse_cost = sch.C[sch.at(steps, s)];
+    if(after_forward_cost) *after_forward_cost = sch.D[sch.at(steps, s)];
+  });
+}
+
+of_status of_adjoint_gradient_binomial(of_ctx* ctx, const of_step_params* prm, int steps,
+                                       int snapshots, const double* target_u,
+                                       const double* target_v, const double* target_w,
+                                       double* grad_u, double* grad_v, double* grad_w,
+                                       of_adjoint_info* info) {
+  return guarded([&] {
+    require_ctx(ctx);
+    require_ptr(prm, "step parameters");
+    const double* tin[3] = {target_u, target_v, target_w};
+    double* gout[3] = {grad_u, grad_v, grad_w};
+    for(int c = 0; c < 3; ++c) {
+      require_ptr(tin[c], "target velocity");
+      require_ptr(gout[c], "gradient output");
+    }
+    if(steps < 1) fail(OF_INVALID_ARGUMENT, "the adjoint run needs at least one step");
+    if(steps > kMaxBinomialSteps)
+      fail(OF_INVALID_ARGUMENT, "the binomial schedule supports 1 to 4096 steps");
+    if(snapshots < 0) fail(OF_INVALID_ARGUMENT, "snapshots must be non-negative");
+    require_adjoint_case(ctx, prm);
+    const std::string name = prm->solver_name ? prm->solver_name : "Taylor-Green";
+    // the pressure and ADI plans exist before the snapshots are sized
+    ctx->poisson_for(ctx->pbc);
+    ctx->adi_for(0.5 * prm->viscosity * prm->dt);
+    AdjWork* W = adj_work(ctx, kAdjBinomial, steps, 0, snapshots);
+    adopt_edges(ctx, W);
+    const Schedule sch(steps, W->snapshots);
+    const std::vector<int> spine = sch.spine();
+    const Grid& g = ctx->g;
+    cudaStream_t s = ctx->stream;
+    cudaEvent_t e0, e1, e2;
+    OFB_CHECK(cudaEventCreate(&e0));
+    OFB_CHECK(cudaEventCreate(&e1));
+    OFB_CHECK(cudaEventCreate(&e2));
+    struct EventGuard {
+      cudaEvent_t a, b, c;
+      ~EventGuard() {
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        cudaEventDestroy(c);
+      }
+    } guard{e0, e1, e2};
+    OFB_CHECK(cudaMemsetAsync(W->acc, 0, 4 * sizeof(double), s));
+    // forward run: the initial state and the spine snapshots are saved on the way
+    OFB_CHECK(cudaEventRecord(e0, s));
+    StepState st = resident_state(ctx);
+    size_t next = 0;
+    try {
+      for(int n = 0; n < steps; ++n) {
+        if(n == 0) save_state(ctx, st, W->slots[0]);
+        if(next < spine.size() && spine[next] == n) save_state(ctx, st, W->slots[1 + next++]);
+        StepHooks hk;
+        if(!W->phi.empty()) hk.phi_store = W->phi[n];
+        forward_step(ctx, prm, name, ctx->metrics.step + 1, st, &hk);
+        ctx->metrics.step += 1;
+        ctx->metrics.time += prm->dt;
+      }
+    } catch(...) {
+      set_resident_state(ctx, st);
+      throw;
+    }
+    set_resident_state(ctx, st);
+    OFB_CHECK(cudaEventRecord(e1, s));
+    const size_t in_use = device_in_use();
+    // loss 1/2 |u(T) - target|^2 on the unique entries and its seed
+    for(int c = 0; c < 3; ++c) {
+      ctx->upload(W->target[c], tin[c], 1 + c);
+      zero(ctx, W->lam_vel[c], 1 + c);
+      zero(ctx, W->lam_prev[c], 1 + c);
+    }
+    zero(ctx, W->lam_p, 0);
+    const double* vel_t[3] = {st.vel[0], st.vel[1], st.vel[2]};
+    const double* tgt[3] = {W->target[0], W->target[1], W->target[2]};
+    ofb::launch_loss_seed(g, ctx->bc, vel_t, tgt, W->lam_vel, W->acc, ctx->rb, s);
+    // reverse sweep; the working state borrows the context's scratch halves.
+    // Its steps swap the halves with the work set's buffers, so each buffer
+    // goes back to its owner afterwards (contents are scratch; all four carry
+    // the state's edge ghosts).
+    BinomialSweep sw{ctx, prm, W, &sch, name};
+    double* own_vel[3];
+    double* own_adv[3];
+    double* own_cur[3];
+    double* own_corr[3];
+    for(int c = 0; c < 3; ++c) {
+      sw.ws.vel[c] = own_vel[c] = W->w_vel[c];
+      sw.ws.adv_prev[c] = own_adv[c] = W->w_adv_prev[c];
+      sw.ws.adv_cur[c] = own_cur[c] = ctx->adv_cur[c];
+      sw.ws.corrected[c] = own_corr[c] = ctx->corrected[c];
+    }
+    sw.ws.p = W->w_p;
+    auto give_back = [&] {
+      for(int c = 0; c < 3; ++c) {
+        W->w_vel[c] = own_vel[c];
+        W->w_adv_prev[c] = own_adv[c];
+        ctx->adv_cur[c] = own_cur[c];
+        ctx->corrected[c] = own_corr[c];
+        W->rc_adv[c] = W->rc_corr[c] = nullptr;
+      }
+    };
+    try {
+      sw.run(0, 0, steps, W->snapshots, true);
+    } catch(...) {
+      give_back();
+      throw;
+    }
+    give_back();
+    // the initial state's ghosts were filled from its active entries
+    if(W->slots[0].clean) ofb::launch_velocity_bc_T(g, W->lam_vel[0], W->lam_vel[1], W->lam_vel[2], s);
+    for(int c = 0; c < 3; ++c) {
+      zero(ctx, W->out[c], 1 + c);
+      ofb::launch_axpby_active(g, ofb::kFaceX + c, 1.0, W->lam_vel[c], 0.0, nullptr, W->out[c], s);
+      ctx->download(gout[c], W->out[c], 1 + c);
+    }
+    OFB_CHECK(cudaEventRecord(e2, s));
+    double acc[4];
+    OFB_CHECK(cudaMemcpyAsync(acc, W->acc, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    ctx->sync();
+    if(info != nullptr) {
+      info->loss = acc[0];
+      info->grad_viscosity = acc[1] + 0.5 * prm->dt * acc[2];
+      info->forward_steps = static_cast<int>(steps + sw.forward);
+      float f_ms = 0.0f, b_ms = 0.0f;
+      OFB_CHECK(cudaEventElapsedTime(&f_ms, e0, e1));
+      OFB_CHECK(cudaEventElapsedTime(&b_ms, e1, e2));
+      info->forward_ms = f_ms;
+      info->backward_ms = b_ms;
+      info->device_bytes = W->bytes;
+      info->snapshots = W->snapshots;
+      info->device_bytes_in_use = in_use;
+    }
+  });
+}
+
 of_status of_adjoint_gradient(of_ctx* ctx, const of_step_params* prm, int steps,
                               int checkpoint_every, const double* target_u,
                               const double* target_v, const double* target_w, double* grad_u,
@@ -1240,7 +1674,7 @@ of_status of_adjoint_gradient(of_ctx* ctx, const of_step_params* prm, int steps,
     require_adjoint_case(ctx, prm);
     const std::string name = prm->solver_name ? prm->solver_name : "Taylor-Green";
     const int every = checkpoint_every < steps ? checkpoint_every : steps;
-    AdjWork* W = adj_work(ctx, steps, every);
+    AdjWork* W = adj_work(ctx, kAdjSegments, steps, every);
     adopt_edges(ctx, W);
     const Grid& g = ctx->g;
     cudaStream_t s = ctx->stream;
@@ -1282,6 +1716,7 @@ of_status of_adjoint_gradient(of_ctx* ctx, const of_step_params* prm, int steps,
     }
     set_resident_state(ctx, st);
     OFB_CHECK(cudaEventRecord(e1, s));
+    const size_t in_use = device_in_use();
     // loss 1/2 |u(T) - target|^2 on the unique entries and its seed
     for(int c = 0; c < 3; ++c) {
       zero(ctx, W->lam_vel[c], 1 + c);
@@ -1339,6 +1774,8 @@ of_status of_adjoint_gradient(of_ctx* ctx, const of_step_params* prm, int steps,
       info->forward_ms = f_ms;
       info->backward_ms = b_ms;
       info->device_bytes = W->bytes;
+      info->snapshots = static_cast<int>(W->ckpt.size() + W->seg.size());
+      info->device_bytes_in_use = in_use;
     }
   });
 }

@@ -49,3 +49,50 @@ def test_no_cpu_fallback_without_gpu():
     import solver_b200.cases as cases
     with pytest.raises(sb.OfError, match="no CUDA device"):
         cases.TaylorGreenCase(cases.TaylorGreenConfig(nx=8, ny=8))
+
+
+def _binom(n, k):
+    from math import comb
+    return comb(n, k) if 0 <= k <= n else 0
+
+
+def _griewank_min_forward_steps(steps, checkpoints):
+    """Least number of forward steps that reverse `steps` steps with
+    `checkpoints` saved states, one of them the initial state (Griewank 1992,
+    Griewank & Walther 2000): t*steps - binom(checkpoints + t, t - 1), t the
+    smallest repetition number with binom(checkpoints + t, t) >= steps."""
+    t = 0
+    while _binom(checkpoints + t, t) < steps:
+        t += 1
+    return t * steps - _binom(checkpoints + t, t - 1)
+
+
+def test_binomial_schedule_cost_is_the_published_minimum():
+    """The C library's schedule (host-only call, no GPU) recomputes exactly the
+    published minimum number of forward steps, and after a forward pass that
+    placed its first snapshots, the recursion restated here."""
+    import solver_b200 as sb
+    for snaps in range(0, 9):
+        for steps in range(1, 121):
+            rev, _ = sb.adjoint_schedule_cost(steps, snaps)
+            s = min(snaps, steps - 1)
+            assert rev == (_griewank_min_forward_steps(steps, s + 1) if steps > 1 else 0), (steps, snaps)
+    # after the forward pass: D(1,s)=0, D(n,0)=n(n-1)/2, D(n,s)=min_m D(n-m,s-1)+C(m,s)
+    N, S = 60, 5
+    C = [[0] * (S + 1) for _ in range(N + 1)]
+    D = [[0] * (S + 1) for _ in range(N + 1)]
+    for n in range(2, N + 1):
+        C[n][0] = D[n][0] = n * (n - 1) // 2
+        for s in range(1, S + 1):
+            C[n][s] = min(m + C[n - m][s - 1] + C[m][s] for m in range(1, n))
+            D[n][s] = min(D[n - m][s - 1] + C[m][s] for m in range(1, n))
+    for n in range(1, N + 1):
+        for s in range(0, S + 1):
+            assert sb.adjoint_schedule_cost(n, s) == (C[n][min(s, n - 1)], D[n][min(s, n - 1)])
+    # the adjoint workloads: 512^3 x 400 steps with 14 snapshots, 128^3 x 100 with 9
+    assert sb.adjoint_schedule_cost(400, 14) == (1047, 650)
+    assert sb.adjoint_schedule_cost(100, 9) == (222, 125)
+    with pytest.raises(ValueError, match="1 to 4096 steps"):
+        sb.adjoint_schedule_cost(4097, 3)
+    with pytest.raises(ValueError, match="non-negative"):
+        sb.adjoint_schedule_cost(10, -1)

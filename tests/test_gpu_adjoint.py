@@ -183,6 +183,40 @@ def test_gradient_independent_of_checkpoint_interval(case):
             1e-12 * abs(grads[0][1]["grad_viscosity"])
 
 
+@pytest.mark.parametrize("snapshots", [0, 1, 2, 3])
+def test_binomial_schedule_gives_the_stored_state_gradient(case, snapshots):
+    """of_adjoint_gradient_binomial reverses 9 steps with 1, 2 or 3 snapshots
+    (recursion of the binomial schedule, the one-snapshot case recomputing
+    from the initial state) or as many as fit (0: all 8): the gradient, the
+    loss and the viscosity derivative equal those of the run that keeps every
+    state (one segment) to rounding (1e-12 relative; the transposed advection
+    scatters with atomics, so two runs of either schedule differ in the last
+    bits), the loss bitwise (it is formed by the forward pass), and the
+    number of forward steps is the schedule's published minimum."""
+    ctx, g, dt, prm, state = case
+    steps = 9
+    w = _direction(g, 23)
+    uT = _forward(ctx, state, prm, steps)
+    target = [uT[i] - w[i] for i in range(3)]
+    upload_initial(ctx, state)
+    ref, ref_info = ctx.adjoint_gradient(prm, steps, target, checkpoint_every=steps)
+    upload_initial(ctx, state)
+    grad, info = ctx.adjoint_gradient_binomial(prm, steps, target, snapshots=snapshots)
+    used = snapshots if snapshots else steps - 1
+    assert info["snapshots"] == used
+    assert info["forward_steps"] == steps + sb.adjoint_schedule_cost(steps, used)[1]
+    gmax = max(float(np.max(np.abs(b))) for b in ref)
+    for a, b in zip(grad, ref):
+        assert np.max(np.abs(a - b)) <= 1e-12 * gmax
+    assert info["loss"] == ref_info["loss"]
+    assert abs(info["grad_viscosity"] - ref_info["grad_viscosity"]) <= \
+        1e-12 * abs(ref_info["grad_viscosity"])
+    # the resident state is left at step `steps`, as of_run_steps leaves it
+    st = ctx.download_state()
+    assert st["metrics"]["step"] == steps
+    assert np.array_equal(st["u"], uT[0])
+
+
 def test_torch_autograd_function_returns_adjoint_gradients(case):
     torch = pytest.importorskip("torch")
     ctx, g, dt, prm, state = case

@@ -275,3 +275,74 @@ def test_mixed_precision_matches_fp64(sb, oracle, n):
     for name in ("u", "v", "w"):
         assert rel_maxdiff(b[name], a[name]) <= 1e-9, name
         assert rel_maxdiff(b[name], getattr(ref, name)) <= 1e-9, name
+
+
+def _host_state(st, pinned):
+    import torch
+    out = {}
+    for name in ("u", "v", "w", "adv_u", "adv_v", "adv_w", "p"):
+        a = np.ascontiguousarray(getattr(st, name) if not isinstance(st, dict) else st[name])
+        if pinned:
+            t = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
+            t.numpy()[...] = a
+            out[name] = t.numpy()
+            out["_keep_" + name] = t
+        else:
+            out[name] = a.copy()
+    return out
+
+
+@pytest.mark.parametrize("pinned", [False, True])
+def test_step_host_equals_upload_step_download(sb, oracle, pinned):
+    """of_step_host (one call per step on host arrays; with pinned arrays the
+    AB2 history comes back while the pressure solve runs) gives bitwise the
+    state of of_state_upload + of_run_steps(1) + of_state_download."""
+    cfg = po.steps_config(32, 32, 16, 0.01, 0.5, 4, 1e-12)
+    g = oracle.tg_grid(cfg)
+    s0 = oracle.tg_init(cfg, 0)
+    prm = sb.step_params(cfg.viscosity, oracle.tg_dt(cfg), cfg.poisson_max_iterations,
+                         cfg.poisson_tolerance)
+    ctx = sb.Context(to_gpu_grid(g), to_gpu_bc(oracle.tg_bc(cfg)))
+    host = _host_state(s0, pinned)
+    host["has_previous_advection"] = 0
+    host["metrics"] = dict(s0.metrics)
+    ref = {k: getattr(s0, k).copy() for k in ("u", "v", "w", "adv_u", "adv_v", "adv_w", "p")}
+    ref_hp, ref_m = 0, dict(s0.metrics)
+    ctx2 = sb.Context(to_gpu_grid(g), to_gpu_bc(oracle.tg_bc(cfg)))
+    for _ in range(4):
+        m = ctx.step_host(prm, host)
+        ctx2.upload_state(ref["u"], ref["v"], ref["w"], ref["adv_u"], ref["adv_v"], ref["adv_w"],
+                          ref["p"], ref_hp, ref_m)
+        ref_m = ctx2.run_steps(prm, 1)
+        st = ctx2.download_state()
+        ref = {k: st[k] for k in ref}
+        ref_hp = st["has_previous_advection"]
+        for name in ref:
+            assert np.array_equal(host[name], ref[name]), name
+        assert host["has_previous_advection"] == ref_hp == 1
+        assert m == ref_m
+    assert m["step"] == 4
+
+
+def test_step_host_failure_leaves_host_state_unchanged(sb, oracle):
+    """A failed step (one CG iteration at tolerance 1e-30) raises like
+    of_run_steps and leaves every host array -- the pinned AB2 history that
+    was being copied back during the step included -- as it was passed in."""
+    cfg = po.steps_config(32, 32, 16, 0.01, 0.5, 2, 1e-12)
+    g = oracle.tg_grid(cfg)
+    s0 = oracle.tg_init(cfg, 0)
+    ctx = sb.Context(to_gpu_grid(g), to_gpu_bc(oracle.tg_bc(cfg)))
+    host = _host_state(s0, True)
+    host["has_previous_advection"] = 0
+    host["metrics"] = dict(s0.metrics)
+    dt = oracle.tg_dt(cfg)
+    ctx.step_host(sb.step_params(cfg.viscosity, dt, cfg.poisson_max_iterations, 1e-12), host)
+    before = {k: host[k].copy() for k in ("u", "v", "w", "adv_u", "adv_v", "adv_w", "p")}
+    assert np.abs(before["adv_u"]).max() > 0
+    with pytest.raises(sb.NotConvergedError,
+                       match="Taylor-Green pressure solve did not converge at step 2"):
+        ctx.step_host(sb.step_params(cfg.viscosity, dt, 1, 1e-30), host)
+    for name, a in before.items():
+        assert np.array_equal(host[name], a), name
+    assert host["has_previous_advection"] == 1
+    assert host["metrics"]["step"] == 1
