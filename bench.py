@@ -590,6 +590,7 @@ def adjoint_long(n=512, steps=400, check_n=256, viscosity=NU, snapshots=0):
     del target
     fwd_ms = info["forward_ms"]
     total_ms = info["forward_ms"] + info["backward_ms"]
+    dt = prm.dt
     check_steps = steps * check_n // n
     ctx, prm, state, target, _ = case(check_n, check_steps, sb.OF_FP64)
     upload_initial(ctx, state)
@@ -605,7 +606,7 @@ def adjoint_long(n=512, steps=400, check_n=256, viscosity=NU, snapshots=0):
         "value": total_ms / fwd_ms, "unit": "x", "higher_is_better": False, "n_gpus": 1,
         "dtype": "f64+f32", "data": "synthetic (Taylor-Green + seeded solenoidal perturbation)",
         "config": {"workload": f"taylor_green_3d_{n}_adjoint", "n": n, "steps": steps,
-                   "viscosity": viscosity, "dt": prm.dt, "poisson_tolerance": TOL,
+                   "viscosity": viscosity, "dt": dt, "poisson_tolerance": TOL,
                    "perturbation": "seed 1, |k| <= 4, RMS 1e-2; target: seed 2 forward run",
                    "schedule": "binomial (optimal revolve), snapshots sized to device memory"},
         "forward_steps_per_s": steps / (fwd_ms / 1000.0),
