@@ -2116,8 +2116,43 @@ __global__ void __launch_bounds__(kTailThreads)
     for(int Q = tid; Q < nc; Q += bd) bc[Q] -= mc;
     __syncthreads();
   }
-  // direct_coarse_solve (:530-567): the host elimination replayed on the rhs
-  {
+  // direct_coarse_solve (:530-567): the host elimination replayed on the rhs.
+  // Up to 32 unknowns (every grid the hierarchy coarsens to 2 per axis) one
+  // warp replays it with the row values in registers, the same operations in
+  // the same order as the block-wide form below, without its two barriers per
+  // pivot and per back-substitution row.
+  if(a.coarse_n <= 32) {
+    const int n = a.coarse_n;
+    if(tid < 32) {
+      constexpr unsigned kFull = 0xffffffffu;
+      const int lane = tid;
+      double yv = lane < n ? double(B(last)[lane]) : 0.0;
+      if(zm && lane == n - 1) yv = 0.0;
+      for(int p = 0; p < n; ++p) {
+        const int sp = a.swaps[p];
+        if(sp != p) {
+          const double at_p = __shfl_sync(kFull, yv, p);
+          const double at_s = __shfl_sync(kFull, yv, sp);
+          if(lane == p) yv = at_s;
+          else if(lane == sp) yv = at_p;
+        }
+        const double yp = __shfl_sync(kFull, yv, p);
+        if(lane > p && lane < n) {
+          const double factor = a.factors[static_cast<size_t>(lane) * n + p];
+          if(factor != 0.0) yv -= factor * yp;
+        }
+      }
+      for(int row = n - 1; row >= 0; --row) {
+        if(lane == row) yv = yv / a.factors[static_cast<size_t>(row) * n + row];
+        const double yr = __shfl_sync(kFull, yv, row);
+        if(lane < row) yv -= a.factors[static_cast<size_t>(lane) * n + row] * yr;
+      }
+      const double sum = __shfl_sync(kFull, warp_sum(lane < n ? yv : 0.0), 0);
+      const double mean = zm ? sum / n : 0.0;
+      if(lane < n) X(last)[lane] = A(yv - mean);
+    }
+    __syncthreads();
+  } else {
     const int n = a.coarse_n;
     A* y = B(last);
     A* xc = X(last);
