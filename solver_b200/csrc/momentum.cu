@@ -19,11 +19,15 @@ __device__ __forceinline__ double tvd_face(double vel, double left, double right
   const bool up = vel >= 0.0;
   const double delta = right - left;
   const double num = up ? left - far_left : far_right - right;
-  // safe_ratio and limiter_value (solver/momentum_terms.cpp:26-40)
-  const double ratio = fabs(delta) < kSmallDenominator ? 0.0 : num / delta;
-  const double a = fabs(ratio);
-  const double phi = (ratio + a) / (1.0 + a);
-  const double muscl = up ? left + 0.5 * phi * delta : right - 0.5 * phi * delta;
+  // safe_ratio and limiter_value (solver/momentum_terms.cpp:26-40) enter as
+  // 0.5 phi(r) delta with r = num / delta (0 when |delta| < 1e-14) and
+  // phi = (r + |r|) / (1 + |r|): zero unless r > 0, and then equal to
+  // num delta / (delta + num) -- one division instead of two; the value
+  // differs from the two-division form by rounding only, the branches not
+  // at all (the sign of r is the product of exact signs).
+  const bool positive = fabs(delta) >= kSmallDenominator && num != 0.0 && ((num > 0.0) == (delta > 0.0));
+  const double half_phi_delta = positive ? num * delta / (delta + num) : 0.0;
+  const double muscl = up ? left + half_phi_delta : right - half_phi_delta;
   const bool first_order = fabs(vel) < kSmallDenominator || (up ? !far_left_ok : !far_right_ok);
   return first_order ? (up ? left : right) : muscl;
 }
