@@ -34,9 +34,12 @@ __device__ __forceinline__ double face_partials(double vel, double left, double 
   const double num = up ? left - far_left : far_right - right;
   const bool tiny = fabs(delta) < kSmallDen;
   const double r = tiny ? 0.0 : num / delta;
-  const double a = fabs(r);
-  const double phi = (r + a) / (1.0 + a);
-  const double dphi = (!tiny && r > 0.0) ? 2.0 / ((1.0 + r) * (1.0 + r)) : 0.0;
+  // phi = (r + |r|) / (1 + |r|) is 0 for r <= 0 and 2 r s for r > 0, with
+  // s = 1 / (1 + r), and phi' = 2 s^2: one division for both
+  const bool positive = !tiny && r > 0.0;
+  const double s = positive ? 1.0 / (1.0 + r) : 0.0;
+  const double phi = 2.0 * r * s;
+  const double dphi = 2.0 * s * s;
   const bool first = fabs(vel) < kSmallDen || (up ? !far_left_ok : !far_right_ok);
   if(first) {
     c[0] = up ? 1.0 : 0.0;

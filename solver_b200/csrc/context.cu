@@ -86,6 +86,7 @@ struct AdjWork {
   std::vector<double*> owned;
   size_t bytes = 0;
   int steps = 0, every = 0, kind = -1, snapshots = 0;
+  bool auto_snapshots = false;  // kAdjBinomial: snapshots sized to the free memory
   // tangent-linear state and the base velocity it is linearised about
   double *t_vel[3] = {}, *t_adv_prev[3] = {}, *t_adv_cur[3] = {}, *t_corr[3] = {}, *t_p = nullptr,
          *base_cur[3] = {};
@@ -561,7 +562,9 @@ constexpr size_t kSnapshotReserve = size_t(2) << 30;  // device memory left free
 AdjWork* adj_work(of_ctx* ctx, int kind, int steps, int every, int snapshots = 0) {
   AdjWork* W = ctx->adj;
   if(W != nullptr && W->kind == kind && W->steps == steps && W->every == every &&
-     (kind != kAdjBinomial || snapshots == 0 || W->snapshots == std::min(snapshots, steps - 1)))
+     (kind != kAdjBinomial ||
+      (snapshots == 0 ? W->auto_snapshots
+                      : !W->auto_snapshots && W->snapshots == std::min(snapshots, steps - 1))))
     return W;
   ctx->sync();
   delete W;
@@ -613,6 +616,7 @@ AdjWork* adj_work(of_ctx* ctx, int kind, int steps, int every, int snapshots = 0
     }
     for(int k = 0; k < want; ++k) W->slots.push_back(alloc_saved(ctx, W));
     W->snapshots = want;
+    W->auto_snapshots = snapshots == 0;
   }
   W->kind = kind;
   W->steps = steps;
