@@ -300,6 +300,56 @@ def test_taylor_green_temporal_self_convergence_gate():
     assert order >= 1.8, (d01, d12, order)
 
 
+# validation/latest/operator_spatial.csv of the reference (its operator MMS
+# tool, 2D periodic sin x cos y on [0, 2 pi]^2): divergence L2 errors
+REF_DIVERGENCE_L2 = {16: 0.00641315, 32: 0.00160561, 64: 0.000401547}
+
+
+def test_operator_spatial_order_gate():
+    """The reference's operator spatial-order gate (validation/
+    run_validation_suite.py:191-275, 515: order >= 1.8 from 16 to 32 to 64;
+    solver/operator_verification.cpp:62-110), run through the GPU path's own
+    operators on the same manufactured fields: the divergence of
+    (sin x cos y, cos x sin y) formed by the projection's pressure rhs
+    (dt = density = 1) against 2 cos x cos y -- equal to the reference's
+    published errors to their printed digits -- and the pressure solve of
+    lap p = -2 sin x cos y against p = sin x cos y (the discrete Laplacian
+    through its inverse).  The velocity field sampled on the faces is a
+    multiple of the discrete gradient of cos x cos y, so its projection must
+    remove it to rounding (gradient, divergence and solve consistent)."""
+    from solver_b200.adjoint import _axis_coords
+    errs = {"div": [], "lap": []}
+    residual = []
+    for n in (16, 32, 64):
+        h = 2.0 * math.pi / n
+        g = sb.Grid(n, n, 1, h, h, 1.0)
+
+        def field(loc, fn):
+            x, y, _ = _axis_coords(g, loc)
+            return np.ascontiguousarray(np.broadcast_to(fn(x[None, None, :], y[None, :, None]),
+                                                        g.shape(loc)))
+        u = field("u", lambda x, y: np.sin(x) * np.cos(y))
+        v = field("v", lambda x, y: np.cos(x) * np.sin(y))
+        w = g.zeros("w")
+        with sb.Context(g, [sb.PERIODIC] * 6) as ctx:
+            out, _, rhs, _ = ctx.project_velocity((u, v, w), 1.0, 1.0, 400, 1e-12)
+            div_exact = field("p", lambda x, y: 2.0 * np.cos(x) * np.cos(y))
+            errs["div"].append(math.sqrt(np.mean((rhs[1, 1:-1, 1:-1] - div_exact[1, 1:-1, 1:-1]) ** 2)))
+            residual.append(math.sqrt(0.5 * (np.mean(out[0][1, 1:-1, 1:-2] ** 2) +
+                                             np.mean(out[1][1, 1:-2, 1:-1] ** 2))))
+            lap = field("p", lambda x, y: -2.0 * np.sin(x) * np.cos(y))
+            p, diag = ctx.solve_pressure_poisson(lap, [sb.P_PERIODIC] * 6, 400, 1e-12)
+            assert diag["converged"]
+            p_exact = field("p", lambda x, y: np.sin(x) * np.cos(y))
+            errs["lap"].append(math.sqrt(np.mean((p[1, 1:-1, 1:-1] - p_exact[1, 1:-1, 1:-1]) ** 2)))
+    for n, e in zip((16, 32, 64), errs["div"]):
+        assert abs(e - REF_DIVERGENCE_L2[n]) <= 1e-5 * REF_DIVERGENCE_L2[n], (n, e)
+    for name, e in errs.items():
+        for a, b in zip(e, e[1:]):
+            assert math.log2(a / b) >= 1.8, (name, e)
+    assert max(residual) <= 1e-12, residual
+
+
 def test_shipped_cavity_128_config_steady_like_the_reference():
     """solver_b200/configs/lid_driven_cavity_re100_128.cfg (Re 100, max |du| <=
     1e-8, Poisson tolerance 1e-8): the reference's build reaches the steady
