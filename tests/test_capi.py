@@ -96,3 +96,18 @@ def test_binomial_schedule_cost_is_the_published_minimum():
         sb.adjoint_schedule_cost(4097, 3)
     with pytest.raises(ValueError, match="non-negative"):
         sb.adjoint_schedule_cost(10, -1)
+
+
+def test_new_entry_points_reject_a_null_context_without_touching_a_device():
+    """The host-state step and the binomial adjoint validate their context
+    before any CUDA call, like every other entry point."""
+    import ctypes as C
+    import solver_b200._capi as capi
+    lib = capi.load()
+    prm = capi.OfStepParams(0.01, 0.01, 1.0, 10, 1e-10, 0, 1, b"Taylor-Green")
+    hp = C.c_int(0)
+    st = lib.of_step_host(None, C.byref(prm), *([None] * 7), C.byref(hp), None)
+    assert st == 1 and lib.of_last_error().decode() == "null context"
+    info = capi.OfAdjointInfo()
+    st = lib.of_adjoint_gradient_binomial(None, C.byref(prm), 4, 0, *([None] * 6), C.byref(info))
+    assert st == 1 and lib.of_last_error().decode() == "null context"
