@@ -301,7 +301,10 @@ of_status of_adjoint_gradient(of_ctx* ctx, const of_step_params* params, int ste
  * Griewank & Walther, ACM TOMS 26, 2000): `snapshots` saved states besides the
  * initial one, placed so that the number of recomputed forward steps is the
  * least possible; snapshots = 0 takes as many as fit in the free device memory
- * (2 GiB kept free, at most 64).  The work set is leaner than
+ * (2 GiB kept free, at most 64), and at most 128 are used in any case (with
+ * 128, no step of a 4096-step horizon is advanced more than twice; the
+ * schedule's dynamic program costs O(steps^2 snapshots) host operations,
+ * about a second at 4096 steps and 128 snapshots).  The work set is leaner than
  * of_adjoint_gradient's (no tangent-linear buffers; the working state shares
  * the context's scratch), which is what lets 512^3 runs of hundreds of steps
  * fit one device.  steps <= 4096.  Every reverse step sees the same
@@ -318,7 +321,8 @@ of_status of_adjoint_gradient_binomial(of_ctx* ctx, const of_step_params* params
  * alone (reverse_cost; Griewank's closed form for snapshots + 1 checkpoints)
  * and right after the forward pass that placed the first snapshots
  * (after_forward_cost, what of_adjoint_gradient_binomial runs beyond its
- * forward pass).  Either pointer may be NULL. */
+ * forward pass).  Snapshots beyond 128 are not used (as above).  Either
+ * pointer may be NULL. */
 of_status of_adjoint_schedule_cost(int steps, int snapshots, long long* reverse_cost,
                                    long long* after_forward_cost);
 
@@ -337,7 +341,9 @@ of_status of_adjoint_schedule_cost(int steps, int snapshots, long long* reverse_
  * cudaMalloc/cudaFree are not acceptable.  The call allocates nothing: its
  * scratch (reduction partials, ticket, norms; 131,104 bytes) is a static
  * device array of the library, found by cudaGetSymbolAddress on the first
- * call on each device (setup; make that first call before any stream capture).
+ * call on each device (setup; make that first call before any stream capture)
+ * and cached until the process exits: do not reset the device
+ * (cudaDeviceReset) between calls.
  *
  *  - u, v, w: device face fields in padded storage whose boundary conditions
  *    are already applied (project_velocity's `working` after

@@ -553,6 +553,11 @@ void keep_pressure_results(of_ctx* ctx, AdjWork* W, int steps) {
 }
 
 constexpr int kMaxSnapshots = 64;
+// The binomial schedule places at most this many snapshots: with 128 free
+// snapshots every one of up to kMaxBinomialSteps = 4096 steps is advanced at
+// most twice in the reverse sweep (binom(131, 2) >= 4096), and the schedule's
+// dynamic program stays near 1e9 cheap operations (it is O(steps^2 snapshots)).
+constexpr int kMaxScheduleSnapshots = 128;
 constexpr size_t kSnapshotReserve = size_t(2) << 30;  // device memory left free by the auto sizing
 
 // Work set of a tangent-linear or adjoint run; kept on the context while the
@@ -607,7 +612,7 @@ AdjWork* adj_work(of_ctx* ctx, int kind, int steps, int every, int snapshots = 0
   } else if(kind == kAdjBinomial) {
     W->slots.push_back(alloc_saved(ctx, W));  // the initial state
     if(steps > 1) keep_pressure_results(ctx, W, steps);
-    int want = std::min(steps - 1, snapshots > 0 ? snapshots : kMaxSnapshots);
+    int want = std::min(steps - 1, snapshots > 0 ? std::min(snapshots, kMaxScheduleSnapshots) : kMaxSnapshots);
     if(snapshots == 0) {
       size_t free_b = 0, total_b = 0;
       OFB_CHECK(cudaMemGetInfo(&free_b, &total_b));
@@ -1394,22 +1399,37 @@ struct Schedule {
   int n = 0, s = 0;
   std::vector<long long> C, D;
   std::vector<int> Cm, Dm;
-  size_t at(int i, int j) const { return static_cast<size_t>(i) * (s + 1) + j; }
+  // snapshot-major: row j holds C(., j), so the split search reads two rows
+  // contiguously
+  size_t at(int i, int j) const { return static_cast<size_t>(j) * (n + 1) + i; }
   Schedule(int steps, int snaps) : n(steps), s(snaps) {
     const size_t size = static_cast<size_t>(n + 1) * (s + 1);
     C.assign(size, 0);
     D.assign(size, 0);
     Cm.assign(size, 0);
     Dm.assign(size, 0);
-    for(int i = 2; i <= n; ++i) {
-      C[at(i, 0)] = D[at(i, 0)] = static_cast<long long>(i) * (i - 1) / 2;
-      for(int j = 1; j <= s; ++j) {
+    for(int i = 2; i <= n; ++i) C[at(i, 0)] = D[at(i, 0)] = static_cast<long long>(i) * (i - 1) / 2;
+    for(int j = 1; j <= s; ++j) {
+      const long long* cj = &C[at(0, j)];
+      const long long* cp = &C[at(0, j - 1)];
+      const long long* dp = &D[at(0, j - 1)];
+      for(int i = 2; i <= n; ++i) {
+        if(j >= i - 1) {
+          // enough snapshots to save every state on the way: advance one step
+          // at a time (C = i - 1; right after the forward pass nothing is left
+          // to advance, D = 0)
+          C[at(i, j)] = i - 1;
+          Cm[at(i, j)] = 1;
+          D[at(i, j)] = 0;
+          Dm[at(i, j)] = 1;
+          continue;
+        }
         long long best_c = -1, best_d = -1;
         int m_c = 1, m_d = 1;
         for(int m = 1; m < i; ++m) {
-          const long long left = C[at(m, j)];
-          const long long c = m + C[at(i - m, j - 1)] + left;
-          const long long d = D[at(i - m, j - 1)] + left;
+          const long long left = cj[m];
+          const long long c = m + cp[i - m] + left;
+          const long long d = dp[i - m] + left;
           if(best_c < 0 || c < best_c) {
             best_c = c;
             m_c = m;
@@ -1521,7 +1541,7 @@ of_status of_adjoint_schedule_cost(int steps, int snapshots, long long* reverse_
     if(steps < 1 || steps > kMaxBinomialSteps)
       fail(OF_INVALID_ARGUMENT, "the binomial schedule supports 1 to 4096 steps");
     if(snapshots < 0) fail(OF_INVALID_ARGUMENT, "snapshots must be non-negative");
-    const int s = std::min(snapshots, std::max(steps - 1, 0));
+    const int s = std::min(std::min(snapshots, kMaxScheduleSnapshots), std::max(steps - 1, 0));
     const Schedule sch(steps, s);
     if(reverse_cost) *reverse_cost = sch.C[sch.at(steps, s)];
     if(after_forward_cost) *after_forward_cost = sch.D[sch.at(steps, s)];

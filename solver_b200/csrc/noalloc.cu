@@ -87,6 +87,9 @@ double* noalloc_scratch() {
   if(g_na_ptr[dev] == nullptr) {
     // First call on this device: the symbol lookup loads this module on the
     // device (if not loaded yet); later calls only read the cached address.
+    // The address stays valid for the life of the process unless the device
+    // is reset (cudaDeviceReset unloads the module), which callers of this
+    // entry point must not do between calls.
     void* p = nullptr;
     OFB_CHECK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
     g_na_ptr[dev] = static_cast<double*>(p);
@@ -104,9 +107,12 @@ void launch_pressure_rhs_noalloc(const Grid& g, const double* u, const double* v
   // the ticket must start at zero; it resets itself, but a launch that never
   // completed would leave it set
   OFB_CHECK(cudaMemsetAsync(ticket, 0, sizeof(unsigned int), s));
-  k_pressure_rhs_noalloc<<<l.grid, l.block, 0, s>>>(g, u, v, w, scale, rhs, scratch + kNaResult,
-                                                    l.kchunk, RedBuf{scratch, ticket});
-  OFB_LAUNCH_CHECK("k_pressure_rhs_noalloc");
+  {
+    ProfScope ps(kKDivergence, s);
+    k_pressure_rhs_noalloc<<<l.grid, l.block, 0, s>>>(g, u, v, w, scale, rhs, scratch + kNaResult,
+                                                      l.kchunk, RedBuf{scratch, ticket});
+    OFB_LAUNCH_CHECK("k_pressure_rhs_noalloc");
+  }
   if(norms_host) {
     OFB_CHECK(cudaMemcpyAsync(norms_host, scratch + kNaResult, 2 * sizeof(double),
                               cudaMemcpyDeviceToHost, s));

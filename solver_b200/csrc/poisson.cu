@@ -24,6 +24,7 @@
 #include "tma.cuh"
 
 #include <cmath>
+#include <cstdint>
 #include <cstdlib>
 #include <cstring>
 #include <algorithm>
@@ -1977,20 +1978,36 @@ __global__ void __launch_bounds__(256)
 // ---------------------------------------------------------------------------
 // The small end of the hierarchy in one block.  From the first level of at
 // most kTailMaxCells cells down to the coarsest, v_cycle (:597-633) runs in
-// one 1024-thread block with every level's rhs, correction and scratch in
-// shared memory, and each mean removal of the reference (after every sweep,
-// on the residual, on the coarse rhs, after the prolongation) done exactly,
-// by a block reduction.  One launch replaces five launches per level, each of
-// which was mostly launch latency and a dependent-load chain.
+// one block with every level's rhs, correction and scratch in shared memory.
+// Each phase ends with one barrier that also publishes the warp partials of
+// the vector it produced; every thread then adds the partials itself (same
+// order in every thread), so the mean of the reference's subtract_active_mean
+// (after every sweep, on the residual, on the coarse rhs, after the
+// prolongation) is known without a second barrier and is subtracted as the
+// next phase loads the vector (a pending shift), as in the per-level kernels.
+// The two pre-sweeps from zero are one phase (k_vsmooth_pre), the
+// prolongation and the first post-sweep another (k_vprolong_smooth).
 // ---------------------------------------------------------------------------
 constexpr int kTailMaxCells = 512;
 constexpr int kTailMaxLevels = 12;
-constexpr int kTailThreads = 256;
+constexpr int kTailThreads = 512;
 
+// Per tail level (all but the coarsest), built on the host when the plan is
+// made and staged into shared memory by every tail launch:
+//   nbr[6][n]   the six operand positions of each cell under the boundary
+//               rules (nb_lo / nb_hi: neighbour, periodic image, or the cell
+//               itself), as +-(index + 1), minus for a homogeneous-Dirichlet
+//               image (ghost = -centre); order x-, x+, y-, y+, z-, z+
+//   parent[n]   the cell's parent on the next coarser level
+//   child[nc][nch]  each coarser cell's children in dz, dy, dx order
+//   dinv[n]     the Jacobi inverse diagonal (T)
+// so a tail phase does no index arithmetic and reads no boundary flags.
 struct TailLevel {
   OpInfo op;
   int sx, sy, sz;  // log2 of the refinement ratio to the next coarser level
   int off;         // offset of the level's b, x, s arrays in shared memory (elements)
+  int tab;         // byte offset of the level's tables in the table region
+  int nch;         // children per coarser cell
 };
 
 struct TailArgs {
@@ -1998,10 +2015,31 @@ struct TailArgs {
   TailLevel lv[kTailMaxLevels];
   int coarse_n;
   int coarse_off;  // offset (elements, 8-byte aligned) of the FP64 solve vector
+  int fact_off;    // offset (8-byte aligned) of the staged factors (coarse_n <= 32)
+  int tab_off;     // byte offset (16-aligned) of the table region in shared memory
+  int tab_bytes;   // its size (a multiple of 16)
+  const unsigned char* tabs;  // the tables in device memory
   const int* swaps;
   const double* factors;
   int zm;
 };
+
+// Byte layout of one tail level's tables (see TailLevel).
+struct TailTabLayout {
+  size_t nbr, parent, child, dinv, bytes;
+};
+
+__host__ __device__ inline size_t align16(size_t v) { return (v + 15) / 16 * 16; }
+
+__host__ __device__ inline TailTabLayout tail_tab_layout(int n, int nc, int nch, size_t tsz) {
+  TailTabLayout t;
+  t.nbr = 0;
+  t.parent = 12 * static_cast<size_t>(n);
+  t.child = t.parent + 2 * static_cast<size_t>(n);
+  t.dinv = align16(t.child + 2 * static_cast<size_t>(nc) * nch);
+  t.bytes = align16(t.dinv + tsz * n);
+  return t;
+}
 
 // Block-wide sum; every thread gets the same total (fixed order).  red has
 // 33 entries: the warp partials and the total.
@@ -2020,116 +2058,142 @@ __device__ __forceinline__ double tail_sum(double v, double* red) {
   return red[32];
 }
 
-__device__ __forceinline__ void tail_coords(const CLay& L, int q, int& i, int& j, int& k) {
-  k = q / L.nxy;
-  const int r = q - k * L.nxy;
-  j = r / L.nx;
-  i = r - j * L.nx;
-}
-
-// smooth_jacobi, one sweep: x <- x + omega (b - A x) / D, then x - mean(x).
-template <typename A>
-__device__ void tail_sweep(const OpInfo& o, const A* b, A* x, A* s, int zm, double* red) {
-  const int n = o.L.count();
-  double part = 0.0;
-  for(int q = threadIdx.x; q < n; q += blockDim.x) {
-    int i, j, k;
-    tail_coords(o.L, q, i, j, k);
-    const ColNb nb = col_nb(o, i, j);
-    A c;
-    const A ax = apply_op<A>(o, nb, i, j, k, [&](int ii, int jj, int kk) { return x[o.L.idx(ii, jj, kk)]; }, c);
-    const A v = c + A(kOmega) * (b[q] - ax) * A(inv_diag(o, i, j, k));
-    s[q] = v;
-    part += double(v);
-  }
-  const double sum = tail_sum(part, red);
-  const A mean = zm ? A(sum / n) : A(0);
-  for(int q = threadIdx.x; q < n; q += blockDim.x) x[q] = s[q] - mean;
+// Ends a tail phase: the block barrier, with the block-wide sum of v (warp
+// partials alternate between two rows of red so that a fast thread's next
+// phase never overwrites partials a slow thread is still adding).
+__device__ __forceinline__ double tail_phase_sum(double v, double (*red)[32], int& par) {
+  v = warp_sum(v);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if(lane == 0) red[par][warp] = v;
   __syncthreads();
+  const int nw = blockDim.x >> 5;
+  double t = 0.0;
+  for(int w = 0; w < nw; ++w) t += red[par][w];
+  par ^= 1;
+  return t;
 }
 
+// One operand value through a table entry e = +-(index + 1).
+template <typename A, typename Op>
+__device__ __forceinline__ A tab_nb(int e, Op op) {
+  const A v = op(e < 0 ? -e - 1 : e - 1);
+  return e < 0 ? -v : v;
+}
+
+// A u at cell q from the staged neighbour table; c gets u at q.
+template <typename A, typename Op>
+__device__ __forceinline__ A tab_apply(const short* nbr, int n, int q, A ix, A iy, A iz, Op op, A& c) {
+  c = op(q);
+  const A l = tab_nb<A>(nbr[q], op);
+  const A r = tab_nb<A>(nbr[n + q], op);
+  const A d = tab_nb<A>(nbr[2 * n + q], op);
+  const A u = tab_nb<A>(nbr[3 * n + q], op);
+  const A b = tab_nb<A>(nbr[4 * n + q], op);
+  const A f = tab_nb<A>(nbr[5 * n + q], op);
+  const A two_c = A(2) * c;
+  return -(r - two_c + l) * ix - (u - two_c + d) * iy - (f - two_c + b) * iz;
+}
+
+// The whole tail V-cycle in the calling block: b_in (shift sb) in, x_out
+// (mean removed) out; sm is the tail's shared-memory layout (TailArgs).
 template <typename T>
-__global__ void __launch_bounds__(kTailThreads)
-    k_vcycle_tail(TailArgs a, const T* __restrict__ b_in, const double* sb_ptr, T* __restrict__ x_out,
-                  LevelScalars* ls_out) {
+__device__ void vcycle_tail_body(const TailArgs& a, const T* __restrict__ b_in, double sb,
+                                 T* __restrict__ x_out, T* sm) {
   using A = T;
-  extern __shared__ __align__(16) unsigned char tail_smem[];
-  A* sm = reinterpret_cast<A*>(tail_smem);
-  __shared__ double red[33];
+  __shared__ double red[2][32];
+  int par = 0;
   const int tid = threadIdx.x, bd = blockDim.x;
   const int zm = a.zm;
+  const A om = A(kOmega);
   auto B = [&](int l) { return sm + a.lv[l].off; };
   auto X = [&](int l) { return sm + a.lv[l].off + a.lv[l].op.L.count(); };
   auto S = [&](int l) { return sm + a.lv[l].off + 2 * a.lv[l].op.L.count(); };
+  unsigned char* tabs = reinterpret_cast<unsigned char*>(sm) + a.tab_off;
+  const int last = a.count - 1;
+  const int nco = a.coarse_n;
+  double* fact = reinterpret_cast<double*>(sm + a.fact_off);
+  int* swp = reinterpret_cast<int*>(fact + (nco <= 32 ? nco * nco : 0));
+  if(nco <= 32) {
+    // the coarse factors, read by the one-warp elimination below
+    for(int q = tid; q < nco * nco; q += bd) fact[q] = a.factors[q];
+    for(int q = tid; q < nco; q += bd) swp[q] = a.swaps[q];
+  }
   {
-    const double sb = *sb_ptr;
+    const uint4* src = reinterpret_cast<const uint4*>(a.tabs);
+    uint4* dst = reinterpret_cast<uint4*>(tabs);
+    for(int q = tid; q < a.tab_bytes / 16; q += bd) dst[q] = __ldg(&src[q]);
     const int n0 = a.lv[0].op.L.count();
     for(int q = tid; q < n0; q += bd) B(0)[q] = A(double(b_in[q]) - sb);
   }
   __syncthreads();
-  const int last = a.count - 1;
-  // descent: pre-smoothing from zero, residual, restriction
+  double sbs[kTailMaxLevels], sxs[kTailMaxLevels];
+  sbs[0] = 0.0;
+  // descent
   for(int l = 0; l < last; ++l) {
-    const OpInfo& o = a.lv[l].op;
-    const int n = o.L.count();
-    A* b = B(l);
+    const TailLevel& tl = a.lv[l];
+    const int n = tl.op.L.count();
+    const int nc = a.lv[l + 1].op.L.count();
+    const TailTabLayout lay = tail_tab_layout(n, nc, tl.nch, sizeof(T));
+    const short* nbr = reinterpret_cast<const short*>(tabs + tl.tab + lay.nbr);
+    const short* child = reinterpret_cast<const short*>(tabs + tl.tab + lay.child);
+    const A* dinv = reinterpret_cast<const A*>(tabs + tl.tab + lay.dinv);
+    const A ix = A(tl.op.inv2[0]), iy = A(tl.op.inv2[1]), iz = A(tl.op.inv2[2]);
+    const A* b = B(l);
     A* x = X(l);
     A* s = S(l);
-    for(int q = tid; q < n; q += bd) x[q] = A(0);
-    __syncthreads();
-    tail_sweep<A>(o, b, x, s, zm, red);
-    tail_sweep<A>(o, b, x, s, zm, red);
+    const A sbl = A(sbs[l]);
+    // both pre-sweeps from a zero correction
     double part = 0.0;
     for(int q = tid; q < n; q += bd) {
-      int i, j, k;
-      tail_coords(o.L, q, i, j, k);
-      const ColNb nb = col_nb(o, i, j);
       A c;
-      const A ax = apply_op<A>(o, nb, i, j, k, [&](int ii, int jj, int kk) { return x[o.L.idx(ii, jj, kk)]; }, c);
-      const A r = b[q] - ax;
-      s[q] = r;
-      part += double(r);
+      const A ax = tab_apply<A>(nbr, n, q, ix, iy, iz, [&](int p) { return om * (b[p] - sbl) * dinv[p]; }, c);
+      const A v = c + om * ((b[q] - sbl) - ax) * dinv[q];
+      x[q] = v;
+      part += double(v);
     }
-    const double rsum = tail_sum(part, red);
-    const A mr = zm ? A(rsum / n) : A(0);
+    {
+      const double t = tail_phase_sum(part, red, par);
+      sxs[l] = zm ? t / n : 0.0;
+    }
+    // residual (b - sb) - A (x - sx)
+    const A sxl = A(sxs[l]);
+    for(int q = tid; q < n; q += bd) {
+      A c;
+      const A ax = tab_apply<A>(nbr, n, q, ix, iy, iz, [&](int p) { return x[p] - sxl; }, c);
+      s[q] = (b[q] - sbl) - ax;
+    }
+    __syncthreads();
     // restrict_full_weighting (:397-424), children in dz, dy, dx order
-    const CLay& Lc = a.lv[l + 1].op.L;
-    const int nc = Lc.count();
-    const int RX = 1 << a.lv[l].sx, RY = 1 << a.lv[l].sy, RZ = 1 << a.lv[l].sz;
-    const A inv_children = A(1.0 / double(RX * RY * RZ));
+    const int nch = tl.nch;
+    const A inv_children = A(1.0 / double(nch));
     A* bc = B(l + 1);
-    double pc = 0.0;
+    part = 0.0;
     for(int Q = tid; Q < nc; Q += bd) {
-      int I, J, K;
-      tail_coords(Lc, Q, I, J, K);
       A sum = A(0);
-      for(int dz = 0; dz < RZ; ++dz)
-        for(int dy = 0; dy < RY; ++dy)
-          for(int dx = 0; dx < RX; ++dx)
-            sum += s[o.L.idx(I * RX + dx, J * RY + dy, K * RZ + dz)] - mr;
+      for(int t = 0; t < nch; ++t) sum += s[child[Q * nch + t]];
       const A v = inv_children * sum;
       bc[Q] = v;
-      pc += double(v);
+      part += double(v);
     }
-    const double csum = tail_sum(pc, red);
-    const A mc = zm ? A(csum / nc) : A(0);
-    for(int Q = tid; Q < nc; Q += bd) bc[Q] -= mc;
-    __syncthreads();
+    {
+      const double t = tail_phase_sum(part, red, par);
+      sbs[l + 1] = zm ? t / nc : 0.0;
+    }
   }
-  // direct_coarse_solve (:530-567): the host elimination replayed on the rhs.
-  // Up to 32 unknowns (every grid the hierarchy coarsens to 2 per axis) one
-  // warp replays it with the row values in registers, the same operations in
-  // the same order as the block-wide form below, without its two barriers per
-  // pivot and per back-substitution row.
-  if(a.coarse_n <= 32) {
-    const int n = a.coarse_n;
+  // direct_coarse_solve (:530-567): the host elimination replayed on the rhs
+  // (its mean removed first, as the reference does before the solve).  Up to
+  // 32 unknowns (every grid the hierarchy coarsens to 2 per axis) one warp
+  // replays it with the rhs in registers and the factors in shared memory,
+  // the same operations in the same order as the block-wide form below.
+  if(nco <= 32) {
+    const int n = nco;
     if(tid < 32) {
       constexpr unsigned kFull = 0xffffffffu;
       const int lane = tid;
-      double yv = lane < n ? double(B(last)[lane]) : 0.0;
+      double yv = lane < n ? double(B(last)[lane]) - sbs[last] : 0.0;
       if(zm && lane == n - 1) yv = 0.0;
       for(int p = 0; p < n; ++p) {
-        const int sp = a.swaps[p];
+        const int sp = swp[p];
         if(sp != p) {
           const double at_p = __shfl_sync(kFull, yv, p);
           const double at_s = __shfl_sync(kFull, yv, sp);
@@ -2138,14 +2202,14 @@ __global__ void __launch_bounds__(kTailThreads)
         }
         const double yp = __shfl_sync(kFull, yv, p);
         if(lane > p && lane < n) {
-          const double factor = a.factors[static_cast<size_t>(lane) * n + p];
+          const double factor = fact[lane * n + p];
           if(factor != 0.0) yv -= factor * yp;
         }
       }
       for(int row = n - 1; row >= 0; --row) {
-        if(lane == row) yv = yv / a.factors[static_cast<size_t>(row) * n + row];
+        if(lane == row) yv = yv / fact[row * n + row];
         const double yr = __shfl_sync(kFull, yv, row);
-        if(lane < row) yv -= a.factors[static_cast<size_t>(lane) * n + row] * yr;
+        if(lane < row) yv -= fact[lane * n + row] * yr;
       }
       const double sum = __shfl_sync(kFull, warp_sum(lane < n ? yv : 0.0), 0);
       const double mean = zm ? sum / n : 0.0;
@@ -2153,11 +2217,12 @@ __global__ void __launch_bounds__(kTailThreads)
     }
     __syncthreads();
   } else {
-    const int n = a.coarse_n;
+    const int n = nco;
+    __shared__ double cred[33];
     A* y = B(last);
     A* xc = X(last);
     double* yd = reinterpret_cast<double*>(sm + a.coarse_off);  // solve in FP64
-    for(int q = tid; q < n; q += bd) yd[q] = double(y[q]);
+    for(int q = tid; q < n; q += bd) yd[q] = double(y[q]) - sbs[last];
     __syncthreads();
     if(zm && tid == 0) yd[n - 1] = 0.0;
     __syncthreads();
@@ -2184,36 +2249,67 @@ __global__ void __launch_bounds__(kTailThreads)
     }
     double part = 0.0;
     for(int q = tid; q < n; q += bd) part += yd[q];
-    const double sum = tail_sum(part, red);
+    const double sum = tail_sum(part, cred);
     const double mean = zm ? sum / n : 0.0;
     for(int q = tid; q < n; q += bd) xc[q] = A(yd[q] - mean);
     __syncthreads();
   }
-  // ascent: prolongate_and_add (:426-451), mean removal, post-smoothing
+  // ascent: prolongate_and_add (:426-451) + first post-sweep, second post-sweep
+  double sxc = 0.0;  // the coarse correction has its mean removed
   for(int l = last - 1; l >= 0; --l) {
-    const OpInfo& o = a.lv[l].op;
-    const int n = o.L.count();
+    const TailLevel& tl = a.lv[l];
+    const int n = tl.op.L.count();
+    const int nc = a.lv[l + 1].op.L.count();
+    const TailTabLayout lay = tail_tab_layout(n, nc, tl.nch, sizeof(T));
+    const short* nbr = reinterpret_cast<const short*>(tabs + tl.tab + lay.nbr);
+    const short* parent = reinterpret_cast<const short*>(tabs + tl.tab + lay.parent);
+    const A* dinv = reinterpret_cast<const A*>(tabs + tl.tab + lay.dinv);
+    const A ix = A(tl.op.inv2[0]), iy = A(tl.op.inv2[1]), iz = A(tl.op.inv2[2]);
+    const A* b = B(l);
     A* x = X(l);
+    A* s = S(l);
     const A* xc = X(l + 1);
-    const CLay& Lc = a.lv[l + 1].op.L;
+    const A sbl = A(sbs[l]), sxl = A(sxs[l]), sec = A(sxc);
     double part = 0.0;
     for(int q = tid; q < n; q += bd) {
-      int i, j, k;
-      tail_coords(o.L, q, i, j, k);
-      const A v = x[q] + xc[Lc.idx(i >> a.lv[l].sx, j >> a.lv[l].sy, k >> a.lv[l].sz)];
+      A c;
+      const A ax = tab_apply<A>(nbr, n, q, ix, iy, iz,
+                                [&](int p) { return (x[p] - sxl) + (xc[parent[p]] - sec); }, c);
+      const A v = c + om * ((b[q] - sbl) - ax) * dinv[q];
+      s[q] = v;
+      part += double(v);
+    }
+    double sa;
+    {
+      const double t = tail_phase_sum(part, red, par);
+      sa = zm ? t / n : 0.0;
+    }
+    const A saa = A(sa);
+    part = 0.0;
+    for(int q = tid; q < n; q += bd) {
+      A c;
+      const A ax = tab_apply<A>(nbr, n, q, ix, iy, iz, [&](int p) { return s[p] - saa; }, c);
+      const A v = c + om * ((b[q] - sbl) - ax) * dinv[q];
       x[q] = v;
       part += double(v);
     }
-    const double sum = tail_sum(part, red);
-    const A mean = zm ? A(sum / n) : A(0);
-    for(int q = tid; q < n; q += bd) x[q] -= mean;
-    __syncthreads();
-    tail_sweep<A>(o, B(l), x, S(l), zm, red);
-    tail_sweep<A>(o, B(l), x, S(l), zm, red);
+    {
+      const double t = tail_phase_sum(part, red, par);
+      sxc = zm ? t / n : 0.0;
+    }
   }
   const int n0 = a.lv[0].op.L.count();
-  for(int q = tid; q < n0; q += bd) x_out[q] = X(0)[q];
-  if(tid == 0) {
+  const A s0 = A(sxc);
+  for(int q = tid; q < n0; q += bd) x_out[q] = X(0)[q] - s0;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kTailThreads)
+    k_vcycle_tail(TailArgs a, const T* __restrict__ b_in, const double* sb_ptr, T* __restrict__ x_out,
+                  LevelScalars* ls_out) {
+  extern __shared__ __align__(16) unsigned char tail_smem[];
+  vcycle_tail_body<T>(a, b_in, *sb_ptr, x_out, reinterpret_cast<T*>(tail_smem));
+  if(threadIdx.x == 0) {
     ls_out->sx = 0.0;  // the mean is already removed
     ls_out->sum_x = 0.0;
   }
@@ -2581,6 +2677,7 @@ struct PoissonPlan {
   int tail_first = -1;
   TailArgs tail{};
   size_t tail_smem = 0;
+  unsigned char* tail_tabs = nullptr;  // the tail's staged tables (TailLevel)
 };
 
 namespace {
@@ -2700,8 +2797,84 @@ void setup_tail(PoissonPlan* P, size_t tsz) {
     t.coarse_off = static_cast<int>(cursor);
     t.coarse_n = P->coarse_n;
     cursor += static_cast<size_t>(P->coarse_n) * sizeof(double) / tsz;
-    const size_t bytes = cursor * tsz;
+    // staged factors (n^2 doubles) and swaps (n ints) of a coarse solve of
+    // at most 32 unknowns
+    cursor = (cursor + align - 1) / align * align;
+    t.fact_off = static_cast<int>(cursor);
+    if(P->coarse_n <= 32)
+      cursor += (static_cast<size_t>(P->coarse_n) * P->coarse_n * sizeof(double) +
+                 static_cast<size_t>(P->coarse_n) * sizeof(int) + tsz - 1) / tsz;
+    // the staged tables of every level but the coarsest
+    const size_t tab_off = align16(cursor * tsz);
+    std::vector<unsigned char> blob;
+    for(int l = first; l + 1 < nl; ++l) {
+      const Level& lv = P->levels[l];
+      const Level& cv = P->levels[l + 1];
+      TailLevel& tl = t.lv[l - first];
+      const int n = lv.L.count(), nc = cv.L.count();
+      tl.nch = lv.rx * lv.ry * lv.rz;
+      tl.tab = static_cast<int>(blob.size());
+      const TailTabLayout lay = tail_tab_layout(n, nc, tl.nch, tsz);
+      blob.resize(blob.size() + lay.bytes, 0);
+      unsigned char* base = blob.data() + tl.tab;
+      int16_t* nbr = reinterpret_cast<int16_t*>(base + lay.nbr);
+      int16_t* parent = reinterpret_cast<int16_t*>(base + lay.parent);
+      int16_t* child = reinterpret_cast<int16_t*>(base + lay.child);
+      const std::vector<double> tinv = inverse_diagonal_table(lv.g, P->pbc);
+      // nb_lo / nb_hi on the host: neighbour, periodic image or the cell itself,
+      // with -1 for a homogeneous-Dirichlet image
+      auto rule = [&](int a, int c, bool hi, int& cc) {
+        const int N = lv.L.n(a);
+        const bool per = lv.op.periodic[a] != 0;
+        const bool dir = (hi ? lv.op.dir_hi[a] : lv.op.dir_lo[a]) != 0;
+        const bool in = hi ? c < N - 1 : c > 0;
+        cc = in ? (hi ? c + 1 : c - 1) : (per ? (hi ? 0 : N - 1) : c);
+        return (in || per || !dir) ? 1 : -1;
+      };
+      auto cls = [](int c, int N) { return N == 1 ? 3 : (c == 0 ? 1 : (c == N - 1 ? 2 : 0)); };
+      for(int k = 0; k < lv.L.nz; ++k)
+        for(int j = 0; j < lv.L.ny; ++j)
+          for(int i = 0; i < lv.L.nx; ++i) {
+            const int q = lv.L.idx(i, j, k);
+            int cc;
+            int sg = rule(0, i, false, cc);
+            nbr[q] = static_cast<int16_t>(sg * (lv.L.idx(cc, j, k) + 1));
+            sg = rule(0, i, true, cc);
+            nbr[n + q] = static_cast<int16_t>(sg * (lv.L.idx(cc, j, k) + 1));
+            sg = rule(1, j, false, cc);
+            nbr[2 * n + q] = static_cast<int16_t>(sg * (lv.L.idx(i, cc, k) + 1));
+            sg = rule(1, j, true, cc);
+            nbr[3 * n + q] = static_cast<int16_t>(sg * (lv.L.idx(i, cc, k) + 1));
+            sg = rule(2, k, false, cc);
+            nbr[4 * n + q] = static_cast<int16_t>(sg * (lv.L.idx(i, j, cc) + 1));
+            sg = rule(2, k, true, cc);
+            nbr[5 * n + q] = static_cast<int16_t>(sg * (lv.L.idx(i, j, cc) + 1));
+            parent[q] = static_cast<int16_t>(cv.L.idx(i / lv.rx, j / lv.ry, k / lv.rz));
+            const double d = tinv[cls(i, lv.L.nx) + 4 * cls(j, lv.L.ny) + 16 * cls(k, lv.L.nz)];
+            if(tsz == sizeof(float)) reinterpret_cast<float*>(base + lay.dinv)[q] = static_cast<float>(d);
+            else reinterpret_cast<double*>(base + lay.dinv)[q] = d;
+          }
+      for(int K = 0; K < cv.L.nz; ++K)
+        for(int J = 0; J < cv.L.ny; ++J)
+          for(int I = 0; I < cv.L.nx; ++I) {
+            int c = 0;
+            const int Q = cv.L.idx(I, J, K);
+            for(int dz = 0; dz < lv.rz; ++dz)
+              for(int dy = 0; dy < lv.ry; ++dy)
+                for(int dx = 0; dx < lv.rx; ++dx)
+                  child[Q * tl.nch + c++] =
+                      static_cast<int16_t>(lv.L.idx(I * lv.rx + dx, J * lv.ry + dy, K * lv.rz + dz));
+          }
+    }
+    t.tab_off = static_cast<int>(tab_off);
+    t.tab_bytes = static_cast<int>(blob.size());
+    const size_t bytes = tab_off + blob.size();
     if(bytes > kSmemLimit) continue;
+    if(!blob.empty()) {
+      OFB_CHECK(cudaMalloc(&P->tail_tabs, blob.size()));
+      OFB_CHECK(cudaMemcpy(P->tail_tabs, blob.data(), blob.size(), cudaMemcpyHostToDevice));
+    }
+    t.tabs = P->tail_tabs;
     t.swaps = P->swaps;
     t.factors = P->factors;
     t.zm = P->zero_mean;
@@ -2983,6 +3156,7 @@ void poisson_plan_destroy(PoissonPlan* P) {
   cudaFree(P->p32b);
   cudaFree(P->sc_in);
   cudaFree(P->fault);
+  cudaFree(P->tail_tabs);
   delete P;
 }
 
@@ -3487,6 +3661,9 @@ void solve_dc(PoissonPlan* P, int max_iterations, double tolerance, SolveScalars
 void poisson_solve(PoissonPlan* P, int max_iterations, double tolerance, SolveScalars* sc_dev,
                    SolveScalars* sc_host, RedBuf rb, cudaStream_t s, double* history,
                    int history_cap) {
+  // the fault word describes this solve only: a wait that gave up in an
+  // earlier solve does not fail the next one
+  OFB_CHECK(cudaMemsetAsync(P->fault, 0, sizeof(int), s));
   if(P->precision == 1)
     solve_dc<float>(P, max_iterations, tolerance, sc_dev, sc_host, rb, s, history, history_cap);
   else

@@ -1,0 +1,186 @@
+"""GPU parity at the sizes and kernel shapes the benchmark runs.
+
+The small parity cases (tests/test_gpu_parity.py) stop at 64 cells per axis.
+The benchmark's 256^3 step runs kernels only wider levels reach: the
+plane-pipelined V-cycle and A p kernels on 256- and 128-wide levels (row
+tiles of 4 and 8 rows, the persistent segment schedule, the 2x2x2
+prolongation from a 128-wide level), the coarse-level engine below them, and
+the warp-scan ADI on 256-long lines.  These tests compare those paths with
+the CPU oracle and with the reference's own build (oracle/_ref):
+
+* periodic Taylor-Green on 256x16x8, 256x32x32 and 128x64x32, 3 steps, FP64
+  and mixed, against the oracle;
+* the 2D Taylor-Green case of the benchmark suite (128^2, viscosity 0.01,
+  CFL 0.5, 100 steps, tolerance 1e-12, u = sin x cos y phase), against the
+  oracle;
+* 3D Taylor-Green at Re 1600, CFL 0.5, tolerance 1e-12 at 128^3 (3 steps)
+  and 256^3 (2 steps: the Euler first step and one AB2 step), FP64 and mixed,
+  against the reference build (solver/taylor_green.cpp:577-633);
+* the Re 100 lid-driven cavity at 1024^2, its first 20 steps, against the
+  reference build (solver/lid_driven_cavity.cpp:562-623).
+
+The reference-build runs take minutes on one core; conftest.py starts them
+in the background when the session starts (tests/refjob.py).
+
+Tolerances: FP64 max-norm relative difference <= 1e-11 for the velocity
+and the AB2 history (vector fields: the largest difference over their three
+components relative to the field's largest component value) and for the
+pressure, equal pressure iteration counts; the mixed path (FP32 V-cycle and
+inner CG inside FP64 defect correction) <= 1e-9.  Per component the
+differences are reported too: in the first Taylor-Green steps w and its
+advection term are still ~1e-4 of u, so a rounding-level difference there is
+small against the vector field but not against w's own maximum.
+On these Taylor-Green grids the cells are anisotropic (the box is
+[0, 2 pi]^3 whatever the cell counts: cells 2-4 times longer in y or z than
+in x on 128x64x32, 8-32 times on the 256-wide ones), so the reference's
+damped-Jacobi V-cycle is a weak preconditioner and CG needs 25-110
+iterations per step.  After that many iterations the residual histories of
+two correct implementations that sum in different orders separate at the
+1e-13 level (measured: the previous per-level kernels and the cooperative
+coarse-level kernel both end steps one iteration before or after the oracle
+with relative residuals 8e-13 .. 1e-12), so there the counts agree to 5 %
+and the fields still to 1e-11.  The isotropic 128^3 and 256^3 runs keep
+exact counts.  On the 32:1 grid (256x16x8) the mixed path's FP32 inner
+solves do not reach the 1e-12 outer tolerance in 400 iterations, so that
+grid is checked in FP64 only.
+"""
+import numpy as np
+import pytest
+
+import pyoracle as po
+import refjob
+from conftest import rel_maxdiff, to_gpu_bc, to_gpu_grid
+
+pytestmark = pytest.mark.gpu
+
+STEP_TOL = 1e-11
+MIXED_TOL = 1e-9
+FIELDS = ("u", "v", "w", "p", "adv_u", "adv_v", "adv_w")
+
+
+@pytest.fixture(scope="module")
+def sb():
+    import solver_b200
+    return solver_b200
+
+
+def _gpu_steps(sb, grid, bc, s0, params, steps, precision):
+    ctx = sb.Context(to_gpu_grid(grid), to_gpu_bc(bc), precision=precision)
+    try:
+        ctx.upload_state(s0.u, s0.v, s0.w, s0.adv_u, s0.adv_v, s0.adv_w, s0.p,
+                         s0.has_previous_advection, s0.metrics)
+        m = ctx.run_steps(params, steps)
+        return ctx.download_state(), m
+    finally:
+        ctx.close()
+
+
+def _field(src, name):
+    return np.asarray(src[name] if isinstance(src, dict) else getattr(src, name))
+
+
+def _compare(out, ref, m, ref_metrics, precision, sb, solve_tol, names=FIELDS, its_slack=0.0):
+    tol = STEP_TOL if precision == sb.OF_FP64 else MIXED_TOL
+    comps = {"velocity": [c for c in ("u", "v", "w") if c in names],
+             "advection": [c for c in ("adv_u", "adv_v", "adv_w") if c in names],
+             "pressure": [c for c in ("p",) if c in names]}
+    per_comp, worst, where = {}, {}, {}
+    for field, cs in comps.items():
+        if not cs:
+            continue
+        scale = max(float(np.max(np.abs(po.active(_field(ref, c))))) for c in cs)
+        dmax = 0.0
+        for c in cs:
+            a, b = po.active(_field(out, c)), po.active(_field(ref, c))
+            d = np.abs(a - b)
+            per_comp[c] = float(rel_maxdiff(a, b)) if a.size else 0.0
+            if d.max() > dmax:
+                dmax = float(d.max())
+                at = np.unravel_index(int(np.argmax(d)), d.shape)
+                where[field] = (c, tuple(int(v) for v in at), float(a[at]), float(b[at]))
+        worst[field] = dmax / scale if scale > 0 else dmax
+    assert all(d <= tol for d in worst.values()), (
+        f"relative max differences {worst}; per component {per_comp}; worst entries {where}")
+    assert m["step"] == ref_metrics["step"]
+    if precision == sb.OF_FP64:
+        its, its_ref = m["pressure_iterations"], ref_metrics["pressure_iterations"]
+        assert abs(its - its_ref) <= its_slack * its_ref, (m, ref_metrics)
+        assert abs(m["max_cfl"] - ref_metrics["max_cfl"]) <= 1e-12 * ref_metrics["max_cfl"]
+    assert m["pressure_relative_residual"] <= solve_tol
+    return worst
+
+
+@pytest.mark.parametrize("n,precision", [((256, 16, 8), "fp64"), ((256, 32, 32), "fp64"),
+                                         ((256, 32, 32), "mixed"), ((128, 64, 32), "fp64"),
+                                         ((128, 64, 32), "mixed")])
+def test_wide_level_shapes_match_oracle(sb, oracle, n, precision):
+    """256- and 128-wide fine levels: plane-pipelined kernels with 4- and
+    8-row tiles, the 128-wide coarse level under a 256-wide one, anisotropic
+    coarsening below (2-cell axes stop coarsening)."""
+    prec = sb.OF_FP64 if precision == "fp64" else sb.OF_MIXED
+    cfg = po.steps_config(*n, 1.0 / 1600.0, 0.5, 3, 1e-12)
+    g = oracle.tg_grid(cfg)
+    s0 = oracle.tg_init(cfg, 0)
+    prm = sb.step_params(cfg.viscosity, oracle.tg_dt(cfg), cfg.poisson_max_iterations,
+                         cfg.poisson_tolerance)
+    out, m = _gpu_steps(sb, g, oracle.tg_bc(cfg), s0, prm, 3, prec)
+    ref = oracle.tg_steps(cfg, 3, s0.copy())
+    _compare(out, ref, m, ref.metrics, prec, sb, cfg.poisson_tolerance, its_slack=0.05)
+
+
+def test_taylor_green_2d_128_100_steps_matches_oracle(sb, oracle):
+    """The benchmark suite's 2D case: 128^2 on [0, 2 pi]^2, viscosity 0.01,
+    CFL 0.5 (dt = 0.0122718463), 100 steps, Poisson tolerance 1e-12, with the
+    u = sin x cos y, v = -cos x sin y, p = (cos 2x + cos 2y)/4 phase."""
+    # the shipped config's final time (solver_b200/configs/taylor_green_2d_128.cfg)
+    cfg = po.tg_config(128, 128, 1, 0.01, 0.5, 1.227184630308513, 200, 1e-12)
+    g = oracle.tg_grid(cfg)
+    assert abs(oracle.tg_dt(cfg) - 0.0122718463030851) < 1e-15
+    s0 = oracle.tg_init(cfg, 1)
+    prm = sb.step_params(cfg.viscosity, oracle.tg_dt(cfg), cfg.poisson_max_iterations,
+                         cfg.poisson_tolerance)
+    out, m = _gpu_steps(sb, g, oracle.tg_bc(cfg), s0, prm, 100, sb.OF_FP64)
+    ref = oracle.tg_steps(cfg, 100, s0.copy())
+    _compare(out, ref, m, ref.metrics, sb.OF_FP64, sb, cfg.poisson_tolerance,
+             names=("u", "v", "p", "adv_u", "adv_v"))
+    assert m["step"] == 100
+    assert m["divergence_l2"] <= 1e-10
+
+
+def _reference_run(sb, oracle, refjob_result, name, precision):
+    cfg = refjob.config(name)
+    kind, _, _, steps = refjob.JOBS[name]
+    if kind == "tg":
+        g, bc, dt = oracle.tg_grid(cfg), oracle.tg_bc(cfg), oracle.tg_dt(cfg)
+        prm = sb.step_params(cfg.viscosity, dt, cfg.poisson_max_iterations, cfg.poisson_tolerance)
+    else:
+        g, bc, dt = oracle.cavity_grid(cfg), oracle.cavity_bc(cfg), oracle.cavity_dt(cfg)
+        prm = sb.step_params(cfg.lid_velocity / cfg.reynolds, dt, cfg.poisson_max_iterations,
+                             cfg.poisson_tolerance, variant=sb.OF_CORRECTION_CAVITY)
+    s0 = refjob.initial_state(oracle, name)  # the oracle's initial state is the reference's, bit for bit
+    out, m = _gpu_steps(sb, g, bc, s0, prm, steps, precision)
+    ref = refjob_result(name)
+    names = FIELDS if g.nz > 1 else ("u", "v", "p", "adv_u", "adv_v")
+    return _compare(out, ref, m, ref["metrics"], precision, sb, cfg.poisson_tolerance, names=names)
+
+
+@pytest.mark.refjob("tg3d_128_3")
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_taylor_green_128_cubed_matches_reference_build(sb, oracle, refjob_result, precision):
+    prec = sb.OF_FP64 if precision == "fp64" else sb.OF_MIXED
+    _reference_run(sb, oracle, refjob_result, "tg3d_128_3", prec)
+
+
+@pytest.mark.refjob("tg3d_256_2")
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_taylor_green_256_cubed_matches_reference_build(sb, oracle, refjob_result, precision):
+    """The headline workload's grid and physics (Re 1600, CFL 0.5, tolerance
+    1e-12): the first (Euler) step and one AB2 step against the reference's
+    own build."""
+    prec = sb.OF_FP64 if precision == "fp64" else sb.OF_MIXED
+    _reference_run(sb, oracle, refjob_result, "tg3d_256_2", prec)
+
+
+@pytest.mark.refjob("cavity_1024_20")
+def test_cavity_1024_first_20_steps_match_reference_build(sb, oracle, refjob_result):
+    _reference_run(sb, oracle, refjob_result, "cavity_1024_20", sb.OF_FP64)

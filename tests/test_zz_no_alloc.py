@@ -121,3 +121,36 @@ def test_noalloc_rejects_oversized_plane():
     st = lib.of_pressure_rhs_noalloc(C.byref(g), 0.0, 1.0, fake, fake, fake, fake, None, None)
     assert st == _capi.OF_INVALID_ARGUMENT
     assert lib.of_last_error().decode() == "build_pressure_rhs expects dt > 0"
+
+
+@pytest.mark.gpu
+def test_noalloc_calls_allocate_no_device_memory(oracle):
+    """The property the entry point exists for: after a first call (which
+    looks up the scratch address and loads the kernel), further calls leave
+    the device's free memory unchanged."""
+    import torch
+    from solver_b200 import _capi
+    lib = _capi.load()
+    g, types = CASES[0]
+    bc = po.bc_from(types)
+    vel = _consistent_velocity(oracle, g, bc, np.random.default_rng(8))
+    dev = [torch.from_numpy(a).to("cuda:0") for a in vel]
+    rhs = torch.zeros(po.shape(g, "p"), dtype=torch.float64, device="cuda:0")
+    norms = np.zeros(2)
+    grid = _abi_grid(g)
+    stream = torch.cuda.Stream(device="cuda:0")
+
+    def call():
+        st = lib.of_pressure_rhs_noalloc(C.byref(grid), 0.01, 1.0, *[t.data_ptr() for t in dev],
+                                         rhs.data_ptr(), norms.ctypes.data_as(_capi.DP),
+                                         stream.cuda_stream)
+        _capi.check(st)
+
+    call()
+    torch.cuda.synchronize()
+    free_before, _ = torch.cuda.mem_get_info(0)
+    for _ in range(10):
+        call()
+    torch.cuda.synchronize()
+    free_after, _ = torch.cuda.mem_get_info(0)
+    assert free_after == free_before
