@@ -15,7 +15,8 @@ Arms:
   --impl reference        the reference's own CPU implementation of the same
                           step (oracle/_ref, the reference's sources compiled
                           in place; the plain-C oracle port if that build is
-                          absent), one process per host core.
+                          absent): the K timed 256^3 steps run as concurrent
+                          single-thread replicas on the host cores.
 
 The FP64 1-GPU line also carries two measurements of the rest of the
 headline metric (skip with --no-extras): "mixed" -- the mixed path's steps/s
@@ -231,56 +232,134 @@ def cpu_step_seconds(n_sample, steps=1):
     return (time.perf_counter() - t0) / steps, kind
 
 
-def _cpu_worker(args):
-    n_sample, steps = args
-    return cpu_step_seconds(n_sample, steps)[0]
-
-
 def cpu_baseline(n, n_sample=128):
+    """A bounded sample (one step at n_sample^3, ~15 s on one core), extrapolated to
+    n^3 by cell count.  The reference arm (--impl reference) measures n^3 itself."""
     sec, kind = cpu_step_seconds(n_sample, 1)
     scale = (n_sample / n) ** 3
     return {"value": scale / sec, "unit": "steps/s", "cores": 1, "kind": kind,
             "sample": f"1 FP64 step of Taylor-Green {n_sample}^3 (nu=1/1600, CFL 0.5, tol 1e-12) "
-                      f"on 1 core took {sec:.2f} s; scaled by cell count to {n}^3",
-            "seconds_per_sample_step": sec}
+                      f"on 1 core took {sec:.2f} s; value EXTRAPOLATED to {n}^3 by cell count "
+                      f"(x{(n / n_sample) ** 3:g}); bench.py --impl reference measures {n}^3 steps",
+            "seconds_per_sample_step": sec, "extrapolated": True}
+
+
+# Resident memory of one reference replica at 256^3 (the reference's state,
+# its step's work fields and the MG hierarchy, plus this driver's copy of the
+# state): 7.8 GB measured, scaled by cell count for other sizes.
+REF_REPLICA_BYTES_256 = 7.9e9
+
+
+def host_available_bytes():
+    """Host memory this process may use: MemAvailable, capped by the cgroup limit."""
+    avail = None
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    avail = int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    try:
+        with open("/sys/fs/cgroup/memory.max") as f:
+            lim = f.read().strip()
+        if lim != "max":
+            avail = min(avail or int(lim), int(lim))
+    except OSError:
+        pass
+    return avail if avail is not None else 16 * 2 ** 30
+
+
+def reference_config(n):
+    """The workload's TaylorGreenConfig for the reference: the 200-step final time of
+    the shipped 256^3 case, whose dt (the reference's T / ceil(T / dt_max) rule) is
+    exactly the B200 arm's dt."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    return pyoracle.tg_config(n, n, n, NU, CFL, 200 * tg_dt(n), MAX_IT, TOL)
+
+
+def _ref_replica(n, warm, timed, barrier, out):
+    """One reference replica (spawned process): its own Taylor-Green state, `warm`
+    untimed steps, then -- after every replica is ready -- `timed` steps of the
+    reference's run_taylor_green_steps, one call per step."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    path, _ = cpu_lib_path()
+    lib = pyoracle.Oracle(path)
+    cfg = reference_config(n)
+    assert lib.tg_dt(cfg) == tg_dt(n)
+    s = lib.tg_init(cfg, 0)
+    for _ in range(warm):
+        s = lib.tg_steps(cfg, 1, s)
+    barrier.wait()
+    t0 = time.perf_counter()
+    for _ in range(timed):
+        s = lib.tg_steps(cfg, 1, s)
+    t1 = time.perf_counter()
+    out.put((t0, t1, timed, s.metrics["pressure_iterations"]))
 
 
 def run_reference_arm(args, world, rank):
-    """The reference's CPU step on all host cores (one process per core)."""
+    """The reference's own CPU step of the same 256^3 workload on the host cores.
+
+    The reference is single-threaded, so the K timed steps run as P independent
+    replicas in parallel (P = K when memory allows, else as many as fit in 60 % of
+    the host's available memory, each replica taking its share of the K steps).
+    Each replica first runs its own untimed warm-up steps (the first, Euler step
+    included; together at least W), then all start their timed steps together;
+    the timed region ends when the last replica finishes.  value = K / that wall
+    time, so ms_per_step * K is the measured wall time of the K steps."""
     if rank != 0:
         return 0
     import multiprocessing as mp
     cores = os.cpu_count() or 1
-    n_sample = args.cpu_sample_n
-    scale = (n_sample / args.n) ** 3
+    n = args.n
+    per_replica = REF_REPLICA_BYTES_256 * (n / 256.0) ** 3
+    fit = max(1, int(0.6 * host_available_bytes() // per_replica))
+    P = max(1, min(args.steps, fit))
+    timed = [args.steps // P + (1 if i < args.steps % P else 0) for i in range(P)]
+    warm = max(1, -(-args.warmup // P))
     ctx = mp.get_context("spawn")
-    step_times = []
-    with ctx.Pool(cores) as pool:
-        for i in range(args.warmup + args.steps):
-            t0 = time.perf_counter()
-            pool.map(_cpu_worker, [(n_sample, 1)] * cores)
-            dt = time.perf_counter() - t0
-            if i >= args.warmup:
-                step_times.append(dt)
-    per_step = sum(step_times) / len(step_times)
-    value = cores * scale / per_step
+    barrier = ctx.Barrier(P)
+    out = ctx.Queue()
+    procs = [ctx.Process(target=_ref_replica, args=(n, warm, timed[i], barrier, out)) for i in range(P)]
+    for p in procs:
+        p.start()
+    results = [out.get() for _ in range(P)]
+    for p in procs:
+        p.join()
+    t0 = min(r[0] for r in results)
+    t1 = max(r[1] for r in results)
+    wall = t1 - t0
+    value = args.steps / wall
     _, kind = cpu_lib_path()
-    sample = (f"each step: {cores} concurrent single-thread FP64 Taylor-Green {n_sample}^3 steps "
-              f"(nu=1/1600, CFL 0.5, tol 1e-12), scaled by cell count to {args.n}^3")
+    sample = (f"{args.steps} FP64 steps of Taylor-Green {n}^3 (nu=1/1600, CFL 0.5, dt = "
+              f"{tg_dt(n):.17g}, tol 1e-12; the reference's own run_taylor_green_steps) as {P} "
+              f"concurrent single-thread replicas on {cores} host cores "
+              f"({max(timed)} timed steps on the busiest; {warm} warm-up step(s) each); "
+              f"measured wall time of the {args.steps} steps {wall:.1f} s")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "steps/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1000.0 / value, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (analytic Taylor-Green)",
-        "config": {"workload": f"taylor_green_3d_{args.n}", "n": args.n, "viscosity": NU,
-                   "cfl": CFL, "poisson_tolerance": TOL},
-        "cpu_baseline": {"value": value, "unit": "steps/s", "cores": cores, "kind": kind,
+        "ms_per_step": 1000.0 * wall / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (analytic Taylor-Green initial state)",
+        "config": workload_config(n, "fp64"),
+        "pressure_iterations_last_step": results[0][3],
+        "cpu_baseline": {"value": value, "unit": "steps/s", "cores": min(P, cores), "kind": kind,
                          "sample": sample},
         "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+def workload_config(n, precision):
+    """The `config` object of both arms' lines (the workload, not the implementation)."""
+    return {"workload": f"taylor_green_3d_{n}", "n": n, "viscosity": NU, "cfl": CFL,
+            "dt": tg_dt(n), "poisson_tolerance": TOL, "precision": precision,
+            "parallelism": "replicas1", "l2": "every field > 126 MB L2; no flush"}
 
 
 # ---------------------------------------------------------------------------
@@ -414,10 +493,8 @@ def run_b200_arm(args, world, rank, local):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if args.precision == "fp64" else "f64+f32",
         "data": "synthetic (analytic Taylor-Green initial state)",
-        "config": {"workload": f"taylor_green_3d_{n}", "n": n, "viscosity": NU, "cfl": CFL,
-                   "dt": dt, "poisson_tolerance": TOL, "precision": args.precision,
-                   "parallelism": f"replicas{world}", "l2": "every field > 126 MB L2; no flush",
-                   "pressure_iterations_last_step": metrics["pressure_iterations"]},
+        "config": dict(workload_config(n, args.precision), parallelism=f"replicas{world}"),
+        "pressure_iterations_last_step": metrics["pressure_iterations"],
         "roofline": roofline,
         "step_hbm": step_hbm,
         "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": state_bytes,
@@ -651,7 +728,7 @@ def main():
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")
     if args.cpu_sample_n is None:
-        args.cpu_sample_n = 128 if args.impl == "b200" else 64
+        args.cpu_sample_n = 128
     world, rank, local = dist_setup()
     if args.impl == "reference":
         return run_reference_arm(args, world, rank)

@@ -93,7 +93,7 @@ def _compare(out, ref, m, ref_metrics, precision, sb, solve_tol, names=FIELDS, i
         for c in cs:
             a, b = po.active(_field(out, c)), po.active(_field(ref, c))
             d = np.abs(a - b)
-            per_comp[c] = float(rel_maxdiff(a, b)) if a.size else 0.0
+            per_comp[c] = float(rel_maxdiff(_field(out, c), _field(ref, c)))
             if d.max() > dmax:
                 dmax = float(d.max())
                 at = np.unravel_index(int(np.argmax(d)), d.shape)
