@@ -84,7 +84,7 @@ def smooth_field(grid: Grid, seed, rms=1.0, kmax=4):
 
 def perturbed_taylor_green(ctx: Context, viscosity, dt, seed, rms=1.0e-2, kmax=4,
                            max_iterations=400, tolerance=1.0e-13):
-    """Taylor-Green (the BASELINE phase, u = sin x cos y cos z) plus a seeded
+    """Taylor-Green (the u = sin x cos y cos z phase) plus a seeded
     solenoidal perturbation (smooth_field, then the device's discrete
     projection); returns the padded (u, v, w, p) host arrays."""
     g = ctx.grid

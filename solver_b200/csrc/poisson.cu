@@ -1510,6 +1510,7 @@ __global__ void __launch_bounds__(256)
            const __grid_constant__ CUtensorMap pm1, const __grid_constant__ CUtensorMap ph1,
            const LevelScalars* ls0, V* p0, V* p1, V* __restrict__ ap, V* __restrict__ x,
            SolveScalars* sc, RedBuf rb, int* fault) {
+  using A = V;  // arithmetic of the vector type: FP64, or FP32 on the mixed path's inner solve
   constexpr int CPT = 4;
   constexpr int D = tpap_slots<V>();
   extern __shared__ __align__(128) unsigned char tsm[];
@@ -1561,20 +1562,20 @@ __global__ void __launch_bounds__(256)
   if(threadIdx.x == 0)
     while(next < nload && next < D) issue(next++);
   const int first = sc->first;
-  const double beta = first ? 0.0 : sc->beta;
-  const double sz = ls0->sx, spo = sc->sp;
-  const double alpha_old = sc->alpha, sx = sc->sx;
-  const double ix = o.inv2[0], iy = o.inv2[1], iz = o.inv2[2];
+  const A beta = A(first ? 0.0 : sc->beta);
+  const A sz = A(ls0->sx), spo = A(sc->sp);
+  const A alpha_old = A(sc->alpha), sx = A(sc->sx);
+  const A ix = A(o.inv2[0]), iy = A(o.inv2[1]), iz = A(o.inv2[2]);
   // raw operand z + beta p_old of the 4 cells at slot row fr
-  auto operand = [&](int sl, int fr, double (&v)[CPT]) {
-    double zv[CPT], pv[CPT];
-    tload4<double>(zslot(sl) + fr * NX + i0, zv);
-    tload4<double>(pslot(sl) + fr * NX + i0, pv);
+  auto operand = [&](int sl, int fr, A (&v)[CPT]) {
+    A zv[CPT], pv[CPT];
+    tload4<A>(zslot(sl) + fr * NX + i0, zv);
+    tload4<A>(pslot(sl) + fr * NX + i0, pv);
 #pragma unroll
     for(int t = 0; t < CPT; ++t) v[t] = zv[t] + beta * pv[t];
   };
   auto point = [&](int sl, int fr, int ii) {
-    return double(zslot(sl)[fr * NX + ii]) + beta * double(pslot(sl)[fr * NX + ii]);
+    return A(zslot(sl)[fr * NX + ii]) + beta * A(pslot(sl)[fr * NX + ii]);
   };
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
   int xl, xr;
@@ -1589,22 +1590,22 @@ __global__ void __launch_bounds__(256)
     double sylo, syhi;
     nb_lo(j0, NY, o.periodic[1], o.dir_lo[1], jm, sylo);
     nb_hi(j0 + TY - 1, NY, o.periodic[1], o.dir_hi[1], jp, syhi);
-    auto own = [&](int l, double (&v)[CPT]) {
+    auto own = [&](int l, A (&v)[CPT]) {
       tma::mbar_wait(&bars[l % D], (l / D) & 1, fault, 1);
       operand(l % D, r + 1, v);
       if constexpr(!PER) {
         double zs;
         vst::zrow(sg.kb - 1 + (l - sg.lbase), NZ, o.periodic[2], o.dir_lo[2], o.dir_hi[2], zs);
 #pragma unroll
-        for(int t = 0; t < CPT; ++t) v[t] *= zs;
+        for(int t = 0; t < CPT; ++t) v[t] *= A(zs);
       }
     };
-    double below[CPT], cen[CPT], above[CPT];
+    A below[CPT], cen[CPT], above[CPT];
     own(sg.lbase, below);
     own(sg.lbase + 1, cen);
     // x of the own cells one plane ahead (plain loads, prefetched a step early)
-    double xn[CPT] = {0.0, 0.0, 0.0, 0.0};
-    if(!first) tload4<double>(x + o.L.idx(i0, j, sg.kb), xn);
+    A xn[CPT] = {A(0), A(0), A(0), A(0)};
+    if(!first) tload4<A>(x + o.L.idx(i0, j, sg.kb), xn);
     __syncthreads();
     for(int k = sg.kb; k < sg.ke; ++k) {
       const int c = sg.lbase + 1 + (k - sg.kb);
@@ -1614,30 +1615,30 @@ __global__ void __launch_bounds__(256)
       }
       own(c + 1, above);
       const int sl = c % D;
-      double dn[CPT], up[CPT];
+      A dn[CPT], up[CPT];
       operand(sl, r, dn);
       operand(sl, r + 2, up);
-      double left = point(sl, r + 1, xl), right = point(sl, r + 1, xr);
+      A left = point(sl, r + 1, xl), right = point(sl, r + 1, xr);
       if constexpr(!PER) {
-        const double sd = r == 0 ? sylo : 1.0, su = r == TY - 1 ? syhi : 1.0;
+        const A sd = A(r == 0 ? sylo : 1.0), su = A(r == TY - 1 ? syhi : 1.0);
 #pragma unroll
         for(int t = 0; t < CPT; ++t) {
           dn[t] *= sd;
           up[t] *= su;
         }
-        left *= sxl;
-        right *= sxr;
+        left *= A(sxl);
+        right *= A(sxr);
       }
       // own cells: exact p (with shifts), the deferred x update
-      double zc[CPT], pc[CPT];
-      tload4<double>(zslot(sl) + (r + 1) * NX + i0, zc);
-      tload4<double>(pslot(sl) + (r + 1) * NX + i0, pc);
-      double pn[CPT], apv[CPT];
+      A zc[CPT], pc[CPT];
+      tload4<A>(zslot(sl) + (r + 1) * NX + i0, zc);
+      tload4<A>(pslot(sl) + (r + 1) * NX + i0, pc);
+      A pn[CPT], apv[CPT];
 #pragma unroll
       for(int t = 0; t < CPT; ++t) {
-        const double l = t > 0 ? cen[t - 1] : left;
-        const double rr = t < CPT - 1 ? cen[t + 1] : right;
-        const double two_c = 2.0 * cen[t];
+        const A l = t > 0 ? cen[t - 1] : left;
+        const A rr = t < CPT - 1 ? cen[t + 1] : right;
+        const A two_c = A(2) * cen[t];
         apv[t] = -(rr - two_c + l) * ix - (up[t] - two_c + dn[t]) * iy - (above[t] - two_c + below[t]) * iz;
         pn[t] = first ? zc[t] - sz : (zc[t] - sz) + beta * (pc[t] - spo);
       }
@@ -1645,22 +1646,22 @@ __global__ void __launch_bounds__(256)
       tstore4<V>(p_out + gq, pn);
       tstore4<V>(ap + gq, apv);
       if(!first) {
-        double xv[CPT];
+        A xv[CPT];
 #pragma unroll
         for(int t = 0; t < CPT; ++t) xv[t] = xn[t];
-        if(k + 1 < sg.ke) tload4<double>(x + o.L.idx(i0, j, k + 1), xn);
+        if(k + 1 < sg.ke) tload4<A>(x + o.L.idx(i0, j, k + 1), xn);
 #pragma unroll
         for(int t = 0; t < CPT; ++t) {
           xv[t] = (xv[t] - sx) + alpha_old * (pc[t] - spo);
-          acc[3] += xv[t];
+          acc[3] += double(xv[t]);
         }
         tstore4<V>(x + gq, xv);
       }
 #pragma unroll
       for(int t = 0; t < CPT; ++t) {
-        acc[0] += pn[t];
-        acc[1] += apv[t];
-        acc[2] += pn[t] * apv[t];
+        acc[0] += double(pn[t]);
+        acc[1] += double(apv[t]);
+        acc[2] += double(pn[t]) * double(apv[t]);
         below[t] = cen[t];
         cen[t] = above[t];
       }
@@ -3379,8 +3380,10 @@ void enqueue_pre(PoissonPlan* P, const CGVec<V>& v, SolveScalars* sc, RedBuf rb,
 // path, where it is measurably faster; in FP64 the separate kernels are as
 // fast.  ORCHARD_B200_NO_VEC containing "fuse" keeps the separate kernels.
 bool fused_cg(const PoissonPlan* P) {
-  return P->precision == 1 && P->tma_ap && P->levels[0].tma_prolong && vec_enabled("tma") &&
-         vec_enabled("fuse");
+  const char* f64 = std::getenv("ORCHARD_B200_FUSE64");
+  const bool fp64_fused = f64 != nullptr && f64[0] == '1';
+  return (P->precision == 1 || fp64_fused) && P->tma_ap && P->levels[0].tma_prolong &&
+         vec_enabled("tma") && vec_enabled("fuse");
 }
 
 // The last deferred x update of a fused-step loop.
