@@ -447,7 +447,15 @@ __global__ void __launch_bounds__(32 * LB) k_adi_scan(SweepArgs a, ScanArgs sa,
     c[a2] = c2 + 1;
     return L.idx(c[0], c[1], c[2]) + a.begin * st;
   };
-  auto slot = [&](int l, int q) { return l * S + (q % K) * 32 + q / K; };
+  // element q = pK + j of a line sits at row j, column (p + rot j) mod 32 of
+  // the line's tile.  On x lines a warp stages consecutive q (32 / K
+  // consecutive p per j): the rotation spreads those accesses over all bank
+  // groups and keeps the solve's row accesses (fixed j, lanes p = 0..31) a
+  // permutation.  Other lines stage 16 lines x 2 elements per warp, already
+  // spread by the odd line stride, so they keep rot = 0.
+  const int rot = XLINES ? (K < 32 ? 32 / K : 1) : 0;
+  auto col = [&](int j, int p) { return j * 32 + ((p + rot * j) & 31); };
+  auto slot = [&](int l, int q) { return l * S + col(q % K, q / K); };
   // staged lines; the padding past n is zero
   if(XLINES) {
     bool ok;
@@ -468,14 +476,14 @@ __global__ void __launch_bounds__(32 * LB) k_adi_scan(SweepArgs a, ScanArgs sa,
     double acc = 0.0;
     for(int j = 0; j < K; ++j) {
       const int q = lane * K + j;
-      double r = line[j * 32 + lane];
+      double r = line[col(j, lane)];
       if(q == 0) r += a.rhs_first;
       if(q == n - 1) r += a.rhs_last;
       const double ipq = __ldg(&sa.ip[j * 32 + lane]);
       // f_q = lower_coupling * ip_q with the coupling -(-beta) folded in
       const double f = q == 0 ? 0.0 : -a.lower * ipq;
       acc = j == 0 ? r * ipq : r * ipq + f * acc;
-      line[j * 32 + lane] = acc;  // A_j
+      line[col(j, lane)] = acc;  // A_j
     }
     // inclusive scan of lane maps: val = m at the lane's last unknown
     double val = acc;
@@ -487,15 +495,15 @@ __global__ void __launch_bounds__(32 * LB) k_adi_scan(SweepArgs a, ScanArgs sa,
     double m_in = __shfl_up_sync(0xffffffffu, val, 1);
     if(lane == 0) m_in = 0.0;
     for(int j = 0; j < K; ++j) {
-      const double v = line[j * 32 + lane] + __ldg(&sa.fB[j * 32 + lane]) * m_in;
-      line[j * 32 + lane] = v;  // m_q
+      const double v = line[col(j, lane)] + __ldg(&sa.fB[j * 32 + lane]) * m_in;
+      line[col(j, lane)] = v;  // m_q
     }
     // back substitution, lane-local: x_{pK+j} = C_j + gD_j x_in
     double cacc = 0.0;
     for(int j = K - 1; j >= 0; --j) {
-      const double mq = line[j * 32 + lane];
+      const double mq = line[col(j, lane)];
       cacc = j == K - 1 ? mq : mq - __ldg(&sa.cu[j * 32 + lane]) * cacc;
-      line[j * 32 + lane] = cacc;  // C_j
+      line[col(j, lane)] = cacc;  // C_j
     }
     double bval = cacc;
 #pragma unroll
@@ -507,8 +515,8 @@ __global__ void __launch_bounds__(32 * LB) k_adi_scan(SweepArgs a, ScanArgs sa,
     if(lane == 31) x_in = 0.0;
     double x0 = 0.0, xl = 0.0;
     for(int j = 0; j < K; ++j) {
-      const double x = line[j * 32 + lane] + __ldg(&sa.gD[j * 32 + lane]) * x_in;
-      line[j * 32 + lane] = x;
+      const double x = line[col(j, lane)] + __ldg(&sa.gD[j * 32 + lane]) * x_in;
+      line[col(j, lane)] = x;
       if(j == 0) x0 = x;
       if(j == K - 1) xl = x;
     }
@@ -516,7 +524,7 @@ __global__ void __launch_bounds__(32 * LB) k_adi_scan(SweepArgs a, ScanArgs sa,
       const double first = __shfl_sync(0xffffffffu, x0, 0);
       const double last = __shfl_sync(0xffffffffu, xl, 31);
       const double factor = (first + a.uc_over_gamma * last) * a.inv_den;
-      for(int j = 0; j < K; ++j) line[j * 32 + lane] -= factor * __ldg(&sa.z[j * 32 + lane]);
+      for(int j = 0; j < K; ++j) line[col(j, lane)] -= factor * __ldg(&sa.z[j * 32 + lane]);
     }
   }
   __syncthreads();

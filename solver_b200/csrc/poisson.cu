@@ -760,11 +760,28 @@ __host__ __device__ inline size_t tprolong_bytes(int nx) {
          tround(static_cast<size_t>(ty / 2 + 2) * (nx / 2) * sizeof(T));
 }
 
-template <typename A, typename S>
+// Four consecutive values from shared (or global) memory.  SWAP (FP64 only):
+// lanes 32 bytes apart read their two 16-byte halves in an order that
+// alternates with (lane ^ lane / 4), so that each quarter-warp phase of a
+// 128-bit shared-memory load touches eight distinct 16-byte bank groups
+// instead of four (no 2-way bank conflict); the same values either way, at
+// the cost of a few registers for the lane-dependent select.
+template <typename A, typename S, bool SWAP = false>
 __device__ __forceinline__ void tload4(const S* p, A (&v)[4]) {
   if constexpr(std::is_same_v<S, double>) {
-    const double2 a = *reinterpret_cast<const double2*>(p);
-    const double2 b = *reinterpret_cast<const double2*>(p + 2);
+    double2 a, b;
+    if constexpr(SWAP) {
+      const int lane = threadIdx.x & 31;
+      const int h = (lane ^ (lane >> 2)) & 1;
+      const double2* q = reinterpret_cast<const double2*>(p);
+      const double2 f = q[h];
+      const double2 g = q[h ^ 1];
+      a = h ? g : f;
+      b = h ? f : g;
+    } else {
+      a = *reinterpret_cast<const double2*>(p);
+      b = *reinterpret_cast<const double2*>(p + 2);
+    }
     v[0] = A(a.x);
     v[1] = A(a.y);
     v[2] = A(b.x);
@@ -1063,7 +1080,7 @@ __global__ void __launch_bounds__(1024 / CPT)
   const A ix = A(o.inv2[0]), iy = A(o.inv2[1]), iz = A(o.inv2[2]);
   auto ldrow = [&](const B* p, double (&v)[CPT]) {
     if constexpr(CPT == 4) {
-      tload4<double>(p, v);
+      tload4<double, B, true>(p, v);
     } else {
 #pragma unroll
       for(int t = 0; t < CPT; ++t) v[t] = double(p[t]);
