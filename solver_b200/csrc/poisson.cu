@@ -2006,7 +2006,7 @@ __global__ void __launch_bounds__(256)
 // The two pre-sweeps from zero are one phase (k_vsmooth_pre), the
 // prolongation and the first post-sweep another (k_vprolong_smooth).
 // ---------------------------------------------------------------------------
-constexpr int kTailMaxCells = 512;
+constexpr int kTailMaxCells = 4096;
 constexpr int kTailMaxLevels = 12;
 constexpr int kTailThreads = 512;
 
@@ -2018,7 +2018,9 @@ constexpr int kTailThreads = 512;
 //               image (ghost = -centre); order x-, x+, y-, y+, z-, z+
 //   parent[n]   the cell's parent on the next coarser level
 //   child[nc][nch]  each coarser cell's children in dz, dy, dx order
-//   dinv[n]     the Jacobi inverse diagonal (T)
+//   cls[n]      the cell's boundary class (x + 4 y + 16 z, each 0 interior,
+//               1 first, 2 last, 3 both) and
+//   itab[64]    the Jacobi inverse diagonal of each class (T)
 // so a tail phase does no index arithmetic and reads no boundary flags.
 struct TailLevel {
   OpInfo op;
@@ -2044,7 +2046,7 @@ struct TailArgs {
 
 // Byte layout of one tail level's tables (see TailLevel).
 struct TailTabLayout {
-  size_t nbr, parent, child, dinv, bytes;
+  size_t nbr, parent, child, cls, itab, bytes;
 };
 
 __host__ __device__ inline size_t align16(size_t v) { return (v + 15) / 16 * 16; }
@@ -2054,8 +2056,9 @@ __host__ __device__ inline TailTabLayout tail_tab_layout(int n, int nc, int nch,
   t.nbr = 0;
   t.parent = 12 * static_cast<size_t>(n);
   t.child = t.parent + 2 * static_cast<size_t>(n);
-  t.dinv = align16(t.child + 2 * static_cast<size_t>(nc) * nch);
-  t.bytes = align16(t.dinv + tsz * n);
+  t.cls = t.child + 2 * static_cast<size_t>(nc) * nch;
+  t.itab = align16(t.cls + static_cast<size_t>(n));
+  t.bytes = align16(t.itab + 64 * tsz);
   return t;
 }
 
@@ -2154,7 +2157,9 @@ __device__ void vcycle_tail_body(const TailArgs& a, const T* __restrict__ b_in, 
     const TailTabLayout lay = tail_tab_layout(n, nc, tl.nch, sizeof(T));
     const short* nbr = reinterpret_cast<const short*>(tabs + tl.tab + lay.nbr);
     const short* child = reinterpret_cast<const short*>(tabs + tl.tab + lay.child);
-    const A* dinv = reinterpret_cast<const A*>(tabs + tl.tab + lay.dinv);
+    const unsigned char* cls = tabs + tl.tab + lay.cls;
+    const A* itab = reinterpret_cast<const A*>(tabs + tl.tab + lay.itab);
+    auto dinv = [&](int p) { return itab[cls[p]]; };
     const A ix = A(tl.op.inv2[0]), iy = A(tl.op.inv2[1]), iz = A(tl.op.inv2[2]);
     const A* b = B(l);
     A* x = X(l);
@@ -2164,8 +2169,8 @@ __device__ void vcycle_tail_body(const TailArgs& a, const T* __restrict__ b_in, 
     double part = 0.0;
     for(int q = tid; q < n; q += bd) {
       A c;
-      const A ax = tab_apply<A>(nbr, n, q, ix, iy, iz, [&](int p) { return om * (b[p] - sbl) * dinv[p]; }, c);
-      const A v = c + om * ((b[q] - sbl) - ax) * dinv[q];
+      const A ax = tab_apply<A>(nbr, n, q, ix, iy, iz, [&](int p) { return om * (b[p] - sbl) * dinv(p); }, c);
+      const A v = c + om * ((b[q] - sbl) - ax) * dinv(q);
       x[q] = v;
       part += double(v);
     }
@@ -2281,7 +2286,9 @@ __device__ void vcycle_tail_body(const TailArgs& a, const T* __restrict__ b_in, 
     const TailTabLayout lay = tail_tab_layout(n, nc, tl.nch, sizeof(T));
     const short* nbr = reinterpret_cast<const short*>(tabs + tl.tab + lay.nbr);
     const short* parent = reinterpret_cast<const short*>(tabs + tl.tab + lay.parent);
-    const A* dinv = reinterpret_cast<const A*>(tabs + tl.tab + lay.dinv);
+    const unsigned char* cls = tabs + tl.tab + lay.cls;
+    const A* itab = reinterpret_cast<const A*>(tabs + tl.tab + lay.itab);
+    auto dinv = [&](int p) { return itab[cls[p]]; };
     const A ix = A(tl.op.inv2[0]), iy = A(tl.op.inv2[1]), iz = A(tl.op.inv2[2]);
     const A* b = B(l);
     A* x = X(l);
@@ -2293,7 +2300,7 @@ __device__ void vcycle_tail_body(const TailArgs& a, const T* __restrict__ b_in, 
       A c;
       const A ax = tab_apply<A>(nbr, n, q, ix, iy, iz,
                                 [&](int p) { return (x[p] - sxl) + (xc[parent[p]] - sec); }, c);
-      const A v = c + om * ((b[q] - sbl) - ax) * dinv[q];
+      const A v = c + om * ((b[q] - sbl) - ax) * dinv(q);
       s[q] = v;
       part += double(v);
     }
@@ -2307,7 +2314,7 @@ __device__ void vcycle_tail_body(const TailArgs& a, const T* __restrict__ b_in, 
     for(int q = tid; q < n; q += bd) {
       A c;
       const A ax = tab_apply<A>(nbr, n, q, ix, iy, iz, [&](int p) { return s[p] - saa; }, c);
-      const A v = c + om * ((b[q] - sbl) - ax) * dinv[q];
+      const A v = c + om * ((b[q] - sbl) - ax) * dinv(q);
       x[q] = v;
       part += double(v);
     }
@@ -2868,10 +2875,13 @@ void setup_tail(PoissonPlan* P, size_t tsz) {
             sg = rule(2, k, true, cc);
             nbr[5 * n + q] = static_cast<int16_t>(sg * (lv.L.idx(i, j, cc) + 1));
             parent[q] = static_cast<int16_t>(cv.L.idx(i / lv.rx, j / lv.ry, k / lv.rz));
-            const double d = tinv[cls(i, lv.L.nx) + 4 * cls(j, lv.L.ny) + 16 * cls(k, lv.L.nz)];
-            if(tsz == sizeof(float)) reinterpret_cast<float*>(base + lay.dinv)[q] = static_cast<float>(d);
-            else reinterpret_cast<double*>(base + lay.dinv)[q] = d;
+            base[lay.cls + q] =
+                static_cast<unsigned char>(cls(i, lv.L.nx) + 4 * cls(j, lv.L.ny) + 16 * cls(k, lv.L.nz));
           }
+      for(int c = 0; c < 64; ++c) {
+        if(tsz == sizeof(float)) reinterpret_cast<float*>(base + lay.itab)[c] = static_cast<float>(tinv[c]);
+        else reinterpret_cast<double*>(base + lay.itab)[c] = tinv[c];
+      }
       for(int K = 0; K < cv.L.nz; ++K)
         for(int J = 0; J < cv.L.ny; ++J)
           for(int I = 0; I < cv.L.nx; ++I) {
