@@ -304,7 +304,7 @@ def run_reference_arm(args, world, rank):
     """The reference's own CPU step of the same 256^3 workload on the host cores.
 
     The reference is single-threaded, so the K timed steps run as P independent
-    replicas in parallel (P = K when memory allows, else as many as fit in 60 % of
+    replicas in parallel (P = K when memory allows, else as many as fit in half of
     the host's available memory, each replica taking its share of the K steps).
     Each replica first runs its own untimed warm-up steps (the first, Euler step
     included; together at least W), then all start their timed steps together;
@@ -316,7 +316,7 @@ def run_reference_arm(args, world, rank):
     cores = os.cpu_count() or 1
     n = args.n
     per_replica = REF_REPLICA_BYTES_256 * (n / 256.0) ** 3
-    fit = max(1, int(0.6 * host_available_bytes() // per_replica))
+    fit = max(1, int(0.5 * host_available_bytes() // per_replica))
     P = max(1, min(args.steps, fit))
     timed = [args.steps // P + (1 if i < args.steps % P else 0) for i in range(P)]
     warm = max(1, -(-args.warmup // P))
