@@ -376,6 +376,16 @@ of_status of_profile_reset(void);
 of_status of_profile_read(int id, long long* launches, long long* timed_launches,
                           double* total_ms);
 
+/* Device time of the V-cycle's coarse-level chain (every level below the
+ * finest, as each CG iteration runs it after the finest level's restriction)
+ * inside a CUDA graph: the chain alone is captured once and replayed `reps`
+ * times on the level-1 rhs of the context's last solve (a diagnostic: it
+ * changes no state that a later solve reads).  *us_per_chain = microseconds
+ * per chain, *launches_per_chain = its kernels.  Per-launch event timing
+ * (of_profile_enable) cannot measure these short kernels inside the graph. */
+of_status of_profile_coarse_chain(of_ctx* ctx, int reps, double* us_per_chain,
+                                  int* launches_per_chain);
+
 #ifdef __cplusplus
 }
 #endif

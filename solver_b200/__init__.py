@@ -355,6 +355,15 @@ def profile_read():
     return out
 
 
+def profile_coarse_chain(ctx, reps=200):
+    """(microseconds, kernels) of one V-cycle coarse-level chain (levels 1 ..
+    coarsest) replayed `reps` times from a CUDA graph of that chain alone, on
+    the level-1 rhs of the context's last solve."""
+    us, n = C.c_double(), C.c_int()
+    _capi.check(ctx._lib.of_profile_coarse_chain(ctx._h, int(reps), C.byref(us), C.byref(n)))
+    return us.value, n.value
+
+
 def context_stream(ctx):
     """The context's cudaStream_t as an integer handle."""
     p = C.c_void_p()

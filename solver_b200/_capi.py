@@ -24,7 +24,7 @@ EXPORTED_SYMBOLS = (
     "of_tg_init", "of_run_steps", "of_stream", "of_kernel_class_count", "of_kernel_class_name",
     "of_profile_enable", "of_profile_reset", "of_profile_read", "of_tangent_linear",
     "of_adjoint_gradient", "of_pressure_rhs_noalloc", "of_step_host",
-    "of_adjoint_gradient_binomial", "of_adjoint_schedule_cost",
+    "of_adjoint_gradient_binomial", "of_adjoint_schedule_cost", "of_profile_coarse_chain",
 )
 
 
@@ -133,6 +133,8 @@ def load():
         lib.of_profile_enable.argtypes = [C.c_int]
         lib.of_profile_read.argtypes = [C.c_int, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
                                         C.POINTER(C.c_double)]
+        lib.of_profile_coarse_chain.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double),
+                                                C.POINTER(C.c_int)]
         _lib = lib
     return _lib
 

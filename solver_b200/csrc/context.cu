@@ -882,6 +882,17 @@ of_status of_stream(of_ctx* ctx, void** stream) {
   });
 }
 
+of_status of_profile_coarse_chain(of_ctx* ctx, int reps, double* us_per_chain, int* launches_per_chain) {
+  return guarded([&] {
+    require_ctx(ctx);
+    require_ptr(us_per_chain, "us_per_chain");
+    require_ptr(launches_per_chain, "launches_per_chain");
+    if(reps < 1) throw std::invalid_argument("reps must be >= 1");
+    ofb::PoissonPlan* plan = ctx->poisson_for(ctx->pbc);
+    *us_per_chain = ofb::poisson_time_coarse_chain(plan, ctx->rb, ctx->stream, reps, launches_per_chain);
+  });
+}
+
 of_status of_device_bytes(of_ctx* ctx, size_t* bytes) {
   return guarded([&] {
     require_ctx(ctx);

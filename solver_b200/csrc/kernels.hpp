@@ -142,6 +142,12 @@ double* poisson_x(PoissonPlan* p);  // compact solution
 void poisson_solve(PoissonPlan* p, int max_iterations, double tolerance, SolveScalars* sc_dev,
                    SolveScalars* sc_host, RedBuf rb, cudaStream_t s, double* history,
                    int history_cap);
+// Device time (us) of the V-cycle's coarse-level chain -- levels 1 .. coarsest,
+// as each CG iteration runs it -- replayed `reps` times from a CUDA graph of
+// that chain alone on the level-1 rhs of the last solve (nothing it writes is
+// read before the next solve's V-cycles overwrite it); *launches = kernels per
+// chain.
+double poisson_time_coarse_chain(PoissonPlan* p, RedBuf rb, cudaStream_t s, int reps, int* launches);
 // Writes x - sx into the active entries of a padded pressure field.
 void launch_compact_to_pressure(const Grid& g, const double* x, const SolveScalars* sc,
                                 double* p_padded, cudaStream_t s);

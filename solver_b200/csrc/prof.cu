@@ -29,6 +29,8 @@ struct Profiler {
   std::vector<cudaEvent_t> pool;
   cudaEvent_t cur_start[kKernelCount] = {};
   long long* capture = nullptr;
+  int mute = 0;  // inside a span: launches are counted, not timed one by one
+  cudaEvent_t span_start[kKernelCount] = {};
 };
 
 Profiler& prof() {
@@ -65,17 +67,38 @@ void prof_launch(int id, cudaStream_t s, bool begin, int count) {
   }
   if(begin) {
     p.launches[id] += count;
-    if(!p.enabled) return;
+    if(!p.enabled || p.mute > 0) return;
     cudaEvent_t e = take_event(p);
     cudaEventRecord(e, s);
     p.cur_start[id] = e;
     return;
   }
-  if(!p.enabled || p.cur_start[id] == nullptr) return;
+  if(!p.enabled || p.mute > 0 || p.cur_start[id] == nullptr) return;
   cudaEvent_t e = take_event(p);
   cudaEventRecord(e, s);
   p.pending.push_back(Pending{id, p.cur_start[id], e});
   p.cur_start[id] = nullptr;
+}
+
+void prof_span(int id, cudaStream_t s, bool begin) {
+  Profiler& p = prof();
+  std::lock_guard<std::mutex> lock(p.mu);
+  if(p.capture != nullptr) return;
+  if(begin) {
+    if(p.enabled && p.mute == 0) {
+      cudaEvent_t e = take_event(p);
+      cudaEventRecord(e, s);
+      p.span_start[id] = e;
+    }
+    ++p.mute;
+    return;
+  }
+  --p.mute;
+  if(p.mute > 0 || !p.enabled || p.span_start[id] == nullptr) return;
+  cudaEvent_t e = take_event(p);
+  cudaEventRecord(e, s);
+  p.pending.push_back(Pending{id, p.span_start[id], e});
+  p.span_start[id] = nullptr;
 }
 
 bool prof_enabled() {

@@ -39,6 +39,17 @@ void prof_capture_begin(long long* counts);
 void prof_capture_end();
 void prof_add_counts(const long long* counts, long long times);
 
+// Times a chain of launches with one event pair (class `id`) instead of one
+// pair per launch; the launches inside are still counted by their scopes.
+void prof_span(int id, cudaStream_t s, bool begin);
+
+struct ProfSpan {
+  int id;
+  cudaStream_t s;
+  ProfSpan(int id_, cudaStream_t s_) : id(id_), s(s_) { prof_span(id, s, true); }
+  ~ProfSpan() { prof_span(id, s, false); }
+};
+
 // Brackets `count` kernel launches of one class: counts them and, when timing
 // is on, records an event pair around them on their stream.
 struct ProfScope {
