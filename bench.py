@@ -466,15 +466,15 @@ def run_b200_arm(args, world, rank, local):
     # they are timed as the product runs them, a CUDA graph of the chain
     # replayed on the device (of_profile_coarse_chain).
     coarse = kernels.get("vcycle_coarse_levels")
-    if coarse:
-        chain_us, chain_launches = sb.profile_coarse_chain(ctx, reps=200)
+    if coarse and args.chain_reps > 0:
+        chain_us, chain_launches = sb.profile_coarse_chain(ctx, reps=args.chain_reps)
         if chain_launches:
             vcycles = coarse["launches_per_step"] / chain_launches
             coarse["ms_per_step_host_loop"] = coarse["ms_per_step"]
             coarse["ms_per_step"] = round(chain_us * vcycles / 1000.0, 4)
             coarse["us_per_vcycle"] = round(chain_us, 2)
             coarse["launches_per_vcycle"] = chain_launches
-            coarse["timing"] = ("CUDA graph of one coarse-level chain replayed 200 times, "
+            coarse["timing"] = (f"CUDA graph of one coarse-level chain replayed {args.chain_reps} times, "
                                 "times the V-cycles per step; ms_per_step_host_loop is the "
                                 "per-launch event timing of the host-driven replay")
 
@@ -730,6 +730,8 @@ def main():
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--profile-steps", type=int, default=2)
+    ap.add_argument("--chain-reps", type=int, default=200,
+                    help="graph replays of the coarse-level chain for its device time (0: skip)")
     ap.add_argument("--cpu-sample-n", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",

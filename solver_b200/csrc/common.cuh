@@ -215,13 +215,16 @@ __device__ __forceinline__ void reduce_finish(double (&v)[K], const bool (&is_ma
   if(tid == 0) {
 #pragma unroll
     for(int k = 0; k < K; ++k) rb.partials[k * kMaxBlocks + bid] = v[k];
-    __threadfence();
-    const unsigned int t = atomicAdd(rb.ticket, 1u);
+    // one acquire-release ticket increment at GPU scope: it publishes this
+    // block's partials and, in the last block, makes every other block's
+    // visible (the CTA barrier below passes that on to the block's threads,
+    // which read the partials from L2); cheaper than a full fence pair
+    unsigned int t;
+    asm volatile("atom.add.acq_rel.gpu.u32 %0, [%1], 1;" : "=r"(t) : "l"(rb.ticket) : "memory");
     last = (t == static_cast<unsigned int>(nblocks - 1));
   }
   __syncthreads();
   if(!last) return;
-  __threadfence();
   double w[K];
 #pragma unroll
   for(int k = 0; k < K; ++k) {
