@@ -3398,25 +3398,29 @@ int resident_blocks(const void* kernel, size_t smem, int threads = 256) {
 
 // Grid of a plane-pipeline launch over `tiles` row tiles and `nzu` planes (or
 // coarse planes): a multiple of the tile count (the z-aligned schedule of
-// tsegments) where that keeps at least 95 % of the blocks that fit, else the
-// contiguous ranges (measured at 256^3: the aligned schedule takes k_tsmooth
-// from 92 to 81 us, but costs k_tap, whose 3 blocks per SM round down from
-// 444 to 384, more than its halo rows gain).
-long long tgrid_blocks(const PoissonPlan* P, int tiles, int nzu, int per_sm, int min_units) {
+// tsegments) where the kernel gains from it (`aligned_always`: its halo rows
+// come from L2) or where that keeps at least 95 % of the blocks that fit,
+// else the contiguous ranges.  Measured at 256^3: the aligned schedule takes
+// the FP64 k_tsmooth from 88 to 80 us and k_trestrict from 72 to 68 us
+// although their 2 blocks per SM round down from 296 to 256; k_tprolong (both
+// precisions), the FP32 k_tsmooth and k_tap (3 blocks per SM, 444 -> 384) lose
+// more to the rounding down than they gain.
+long long tgrid_blocks(const PoissonPlan* P, int tiles, int nzu, int per_sm, int min_units,
+                       bool aligned_always) {
   const long long items = static_cast<long long>(tiles) * nzu;
   long long g = std::min<long long>(static_cast<long long>(per_sm) * P->sms, std::max(1LL, items / min_units));
   const long long aligned = tiles * std::min<long long>(nzu, g / tiles);
-  if(aligned > 0 && aligned * 20 >= g * 19) return aligned;
+  if(aligned > 0 && (aligned_always || aligned * 20 >= g * 19)) return aligned;
   while((items / g + 1) / nzu + 2 > kTMaxSeg) ++g;
   if(g % tiles == 0) ++g;  // a multiple of the tile count would select the aligned schedule
   return g;
 }
 
 TGrid tgrid(const PoissonPlan* P, const CLay& L, size_t elem, const void* kernel, size_t smem,
-            int threads = 256) {
+            int threads = 256, bool aligned_always = false) {
   const int ty = 1024 / L.nx;
   const int per_sm = std::min(tper_sm(elem), resident_blocks(kernel, smem, threads));
-  return TGrid{static_cast<int>(tgrid_blocks(P, L.ny / ty, L.nz, per_sm, 4)), ty};
+  return TGrid{static_cast<int>(tgrid_blocks(P, L.ny / ty, L.nz, per_sm, 4, aligned_always)), ty};
 }
 
 // v_cycle (linsolve/poisson_solver.cpp:597-633) from level l; the finest
@@ -3433,19 +3437,19 @@ void v_cycle(PoissonPlan* P, int l, const V* r0, SolveScalars* sc, RedBuf rb, cu
   T* x = static_cast<T*>(lv.x);
   if(l == P->tail_first) {
     ProfScope ps(kKCoarseLevels, s);
-    launch_pdl(P->tail.per ? k_vcycle_tail<T, true> : k_vcycle_tail<T, false>, 1, kTailThreads, P->tail_smem, s,
-               P->tail, static_cast<const T*>(lv.b), &ls->sb, x, ls);
+    launch_pdl(P->tail.per ? k_vcycle_tail<T, true> : k_vcycle_tail<T, false>, 1, kTailThreads, P->tail_smem,
+               s, P->tail, static_cast<const T*>(lv.b), &ls->sb, x, ls);
     OFB_LAUNCH_CHECK("k_vcycle_tail");
     return;
   }
   if(l + 1 == nl) {
     ProfScope ps(kKCoarseSolve, s);
     if(l == 0)
-      launch_pdl(k_coarse_solve<T, V>, 1, 256, 0, s, P->coarse_n, P->swaps, P->factors, r0, sb_ptr, x, ls,
-                                             zm, rz_sc);
+      launch_pdl(k_coarse_solve<T, V>, 1, 256, 0, s, P->coarse_n, P->swaps, P->factors, r0, sb_ptr, x, ls, zm,
+                 rz_sc);
     else
       launch_pdl(k_coarse_solve<T, T>, 1, 256, 0, s, P->coarse_n, P->swaps, P->factors,
-                                            static_cast<const T*>(lv.b), sb_ptr, x, ls, zm, rz_sc);
+                 static_cast<const T*>(lv.b), sb_ptr, x, ls, zm, rz_sc);
     OFB_LAUNCH_CHECK("k_coarse_solve");
     return;
   }
@@ -3473,15 +3477,16 @@ void v_cycle(PoissonPlan* P, int l, const V* r0, SolveScalars* sc, RedBuf rb, cu
     } else {
       {
         ProfScope ps(fine ? kKSmoothFirstFine : kKCoarseLevels, s);
-        launch_pdl(k_smooth_first<T, B>, ln.grid, ln.block, 0, s, lv.op, bptr, sb_ptr, a, ls, zm, ln.kchunk, rb);
+        launch_pdl(k_smooth_first<T, B>, ln.grid, ln.block, 0, s, lv.op, bptr, sb_ptr, a, ls, zm, ln.kchunk,
+                   rb);
       }
       ProfScope ps(fine ? kKSmoothFine : kKCoarseLevels, s);
       if(vsm)
         launch_pdl(k_vsmooth<T, B>, lr.grid, lr.block, 0, s, lv.op, bptr, sb_ptr, a, &ls->sa, x, ls, zm,
-                                                     nullptr, lr.kchunk, rb);
+                   nullptr, lr.kchunk, rb);
       else
         launch_pdl(k_smooth<T, B>, ln.grid, ln.block, 0, s, lv.op, bptr, sb_ptr, a, &ls->sa, x, ls, 1, zm,
-                                                    nullptr, ln.kchunk, rb);
+                   nullptr, ln.kchunk, rb);
     }
     if(lv.tma_prolong && vec_enabled("tma")) {
       ProfScope ps(fine ? kKRestrictFine : kKCoarseLevels, s);
@@ -3489,17 +3494,16 @@ void v_cycle(PoissonPlan* P, int l, const V* r0, SolveScalars* sc, RedBuf rb, cu
       const size_t sm = tslot_bytes<T, B>(lv.L.nx) * kTSlots + static_cast<size_t>(ty) * (lv.L.nx / 2) * sizeof(T);
       const auto kern = P->all_periodic ? k_trestrict<T, B, kTSlots, true> : k_trestrict<T, B, kTSlots, false>;
       const int per_sm = std::min(tper_sm(sizeof(T)), resident_blocks(reinterpret_cast<const void*>(kern), sm));
-      const long long g = tgrid_blocks(P, lv.L.ny / ty, lv.L.nz / 2, per_sm, 2);
-      launch_pdl(kern, static_cast<int>(g), 256, sm, s, lv.op, cv.op, lv.tm_xm, lv.tm_xh, lv.tm_bm, sb_ptr, &ls->sx,
-                                                static_cast<T*>(cv.b), lsc, zm, rb, P->fault);
+      const long long g = tgrid_blocks(P, lv.L.ny / ty, lv.L.nz / 2, per_sm, 2, std::is_same_v<T, double>);
+      launch_pdl(kern, static_cast<int>(g), 256, sm, s, lv.op, cv.op, lv.tm_xm, lv.tm_xh, lv.tm_bm, sb_ptr,
+                 &ls->sx, static_cast<T*>(cv.b), lsc, zm, rb, P->fault);
     } else {
       ProfScope ps(fine ? kKRestrictFine : kKCoarseLevels, s);
       if(vre && lv.rx == 2 && lv.ry == 2 && lv.rz == 2) {
         const vst::RowLaunch lrc =
             vst::row_launch(lv.L.nx, cv.L.ny, cv.L.nz, vst::Width<T>::W, 8);
         launch_pdl(k_vrestrict<T, B>, lrc.grid, lrc.block, 0, s, lv.op, cv.op, bptr, sb_ptr, x, &ls->sx,
-                                                         static_cast<T*>(cv.b), lsc, zm,
-                                                         lrc.kchunk, rb);
+                   static_cast<T*>(cv.b), lsc, zm, lrc.kchunk, rb);
       } else
         launch_restrict<T, B>(lv, cv, bptr, sb_ptr, x, &ls->sx, static_cast<T*>(cv.b), lsc, zm,
                               lc, rb, s);
@@ -3520,34 +3524,35 @@ void v_cycle(PoissonPlan* P, int l, const V* r0, SolveScalars* sc, RedBuf rb, cu
       const size_t sm = tprolong_bytes<T, B>(lv.L.nx) * 4;
       const auto kern = P->all_periodic ? k_tprolong<T, B, 4, 4, true> : k_tprolong<T, B, 4, 4, false>;
       const TGrid tg = tgrid(P, lv.L, sizeof(T), reinterpret_cast<const void*>(kern), sm);
-      launch_pdl(kern, tg.grid, 256, sm, s, lv.op, lv.tm_xm, lv.tm_xh, lv.tm_bm, lv.tm_em, lv.tm_eh, sb_ptr, &ls->sx,
-                                    &lsc->sx, a, ls, zm, rb, P->fault);
+      launch_pdl(kern, tg.grid, 256, sm, s, lv.op, lv.tm_xm, lv.tm_xh, lv.tm_bm, lv.tm_em, lv.tm_eh, sb_ptr,
+                 &ls->sx, &lsc->sx, a, ls, zm, rb, P->fault);
     } else {
       ProfScope ps(fine ? kKProlongFine : kKCoarseLevels, s);
       if(vpr)
-        launch_pdl(k_vprolong_smooth<T, B>, lr.grid, lr.block, 0, s, 
-            lv.op, cv.L, bptr, sb_ptr, x, &ls->sx, static_cast<const T*>(cv.x), &lsc->sx, a, ls,
-            lv.rx == 2 ? 1 : 0, lv.ry == 2 ? 1 : 0, lv.rz == 2 ? 1 : 0, zm, lr.kchunk, rb);
+        launch_pdl(k_vprolong_smooth<T, B>, lr.grid, lr.block, 0, s, lv.op, cv.L, bptr, sb_ptr, x, &ls->sx,
+                   static_cast<const T*>(cv.x), &lsc->sx, a, ls, lv.rx == 2 ? 1 : 0, lv.ry == 2 ? 1 : 0,
+                   lv.rz == 2 ? 1 : 0, zm, lr.kchunk, rb);
       else
-        launch_pdl(k_prolong_smooth<T, B>, ln.grid, ln.block, 0, s, 
-            lv.op, cv.L, bptr, sb_ptr, x, &ls->sx, static_cast<const T*>(cv.x), &lsc->sx, a, ls,
-            lv.rx == 2 ? 1 : 0, lv.ry == 2 ? 1 : 0, lv.rz == 2 ? 1 : 0, zm, ln.kchunk, rb);
+        launch_pdl(k_prolong_smooth<T, B>, ln.grid, ln.block, 0, s, lv.op, cv.L, bptr, sb_ptr, x, &ls->sx,
+                   static_cast<const T*>(cv.x), &lsc->sx, a, ls, lv.rx == 2 ? 1 : 0, lv.ry == 2 ? 1 : 0,
+                   lv.rz == 2 ? 1 : 0, zm, ln.kchunk, rb);
     }
     if(lv.tma && vec_enabled("tma")) {
       ProfScope ps(fine ? kKSmoothFine : kKCoarseLevels, s);
       const size_t sm = tslot_bytes<T, B>(lv.L.nx) * kTSlots;
       const auto kern = P->all_periodic ? k_tsmooth<T, B, 4, true> : k_tsmooth<T, B, 4, false>;
-      const TGrid tg = tgrid(P, lv.L, sizeof(T), reinterpret_cast<const void*>(kern), sm);
-      launch_pdl(kern, tg.grid, 256, sm, s, lv.op, lv.tm_am, lv.tm_ah, lv.tm_bm, sb_ptr, &ls->sa, x, ls, zm, rz_sc, rb,
-                                    P->fault);
+      const TGrid tg =
+          tgrid(P, lv.L, sizeof(T), reinterpret_cast<const void*>(kern), sm, 256, std::is_same_v<T, double>);
+      launch_pdl(kern, tg.grid, 256, sm, s, lv.op, lv.tm_am, lv.tm_ah, lv.tm_bm, sb_ptr, &ls->sa, x, ls, zm,
+                 rz_sc, rb, P->fault);
     } else {
       ProfScope ps(fine ? kKSmoothFine : kKCoarseLevels, s);
       if(vsm)
         launch_pdl(k_vsmooth<T, B>, lr.grid, lr.block, 0, s, lv.op, bptr, sb_ptr, a, &ls->sa, x, ls, zm,
-                                                     rz_sc, lr.kchunk, rb);
+                   rz_sc, lr.kchunk, rb);
       else
         launch_pdl(k_smooth<T, B>, ln.grid, ln.block, 0, s, lv.op, bptr, sb_ptr, a, &ls->sa, x, ls, 1, zm,
-                                                    rz_sc, ln.kchunk, rb);
+                   rz_sc, ln.kchunk, rb);
     }
     OFB_LAUNCH_CHECK("v_cycle ascent");
   };
@@ -3617,8 +3622,8 @@ void enqueue_body(PoissonPlan* P, const CGVec<V>& v, SolveScalars* sc, RedBuf rb
                          tround(static_cast<size_t>(ty + 2) * l0.L.nx * sizeof(V))) * tpap_slots<V>();
       const auto kern = P->all_periodic ? k_tpap<T, V, true> : k_tpap<T, V, false>;
       const TGrid tg = tgrid(P, l0.L, sizeof(V), reinterpret_cast<const void*>(kern), sm);
-      launch_pdl(kern, tg.grid, 256, sm, s, l0.op, l0.tm_xm, l0.tm_xh, P->tm_pm, P->tm_ph, P->tm_pm2, P->tm_ph2, P->ls,
-                                    v.p, v.p2, v.ap, v.x, sc, rb, P->fault);
+      launch_pdl(kern, tg.grid, 256, sm, s, l0.op, l0.tm_xm, l0.tm_xh, P->tm_pm, P->tm_ph, P->tm_pm2,
+                 P->tm_ph2, P->ls, v.p, v.p2, v.ap, v.x, sc, rb, P->fault);
     }
     {
       ProfScope ps(kKUpdateXr, s);
@@ -3632,8 +3637,8 @@ void enqueue_body(PoissonPlan* P, const CGVec<V>& v, SolveScalars* sc, RedBuf rb
   }
   {
     ProfScope ps(kKUpdateP, s);
-    launch_pdl(k_update_p<T, V>, ln.grid, ln.block, 0, s, l0.L, static_cast<const T*>(l0.x), P->ls, v.p,
-                                                  sc, ln.kchunk, rb);
+    launch_pdl(k_update_p<T, V>, ln.grid, ln.block, 0, s, l0.L, static_cast<const T*>(l0.x), P->ls, v.p, sc,
+               ln.kchunk, rb);
   }
   {
     ProfScope ps(kKApplyAp, s);
