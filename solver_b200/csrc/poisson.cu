@@ -828,8 +828,9 @@ struct TSeg {
 
 __device__ __forceinline__ int tsegments(int tiles, int nz, TSeg (&seg)[kTMaxSeg], int& nload) {
   if(gridDim.x % tiles == 0) {
-    // z-aligned schedule (the host picks it whenever the grid covers every
-    // tile): block b owns tile b % tiles and z chunk b / tiles, so the blocks
+    // z-aligned schedule (the host selects it by launching a multiple of the
+    // tile count, tgrid_blocks): block b owns tile b % tiles and z chunk
+    // b / tiles, so the blocks
     // of neighbouring tiles stream the same planes at the same time and a
     // tile's halo rows -- its neighbours' edge rows -- come from L2, not DRAM
     const int nzc = gridDim.x / tiles;
