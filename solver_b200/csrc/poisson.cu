@@ -1068,7 +1068,8 @@ __global__ void __launch_bounds__(1024 / CPT + 32)
   constexpr int D = kTSlots;
   extern __shared__ __align__(128) unsigned char tsm[];
   __shared__ uint64_t bars[D], empt[D];  // slot loaded / slot released
-  __shared__ double invd_s[64];
+  __shared__ A invd_s[64];
+  using L = std::conditional_t<std::is_same_v<T, float>, float, double>;  // loaded rhs values
   const int NX = o.L.nx, NY = o.L.ny, NZ = o.L.nz;
   const int TY = 1024 / NX;
   const int tpr = NX / CPT;
@@ -1104,17 +1105,17 @@ __global__ void __launch_bounds__(1024 / CPT + 32)
     }
     tma::fence_barrier_init();
   }
-  if(threadIdx.x < 64) invd_s[threadIdx.x] = o.invd[threadIdx.x];
+  if(threadIdx.x < 64) invd_s[threadIdx.x] = A(o.invd[threadIdx.x]);
   __syncthreads();
   const double sb = *sb_ptr;
   const A om = A(kOmega);
   const A ix = A(o.inv2[0]), iy = A(o.inv2[1]), iz = A(o.inv2[2]);
-  auto ldrow = [&](const B* p, double (&v)[CPT]) {
+  auto ldrow = [&](const B* p, L (&v)[CPT]) {
     if constexpr(CPT == 4) {
-      tload4<double, B, true>(p, v);
+      tload4<L, B, std::is_same_v<B, double>>(p, v);
     } else {
 #pragma unroll
-      for(int t = 0; t < CPT; ++t) v[t] = double(p[t]);
+      for(int t = 0; t < CPT; ++t) v[t] = L(p[t]);
     }
   };
   double acc[1] = {0.0};
@@ -1164,7 +1165,7 @@ __global__ void __launch_bounds__(1024 / CPT + 32)
       double zs;
       const int kz = vst::zrow(sg.kb - 1 + (l - sg.lbase), NZ, o.periodic[2], o.dir_lo[2], o.dir_hi[2], zs);
       const int cz = 16 * axis_class(kz, NZ);
-      double b[CPT];
+      L b[CPT];
       ldrow(slot(l % D) + (r + 1) * NX + i0, b);
       if constexpr(PER) {
         // raw b: the operator annihilates the constant omega sb / D
@@ -1172,7 +1173,7 @@ __global__ void __launch_bounds__(1024 / CPT + 32)
         for(int t = 0; t < CPT; ++t) v[t] = A(b[t]);
       } else {
 #pragma unroll
-        for(int t = 0; t < CPT; ++t) v[t] = A(zs) * om * A(b[t] - sb) * A(invd_s[cown[t] + cz]);
+        for(int t = 0; t < CPT; ++t) v[t] = A(zs) * om * A(b[t] - L(sb)) * A(invd_s[cown[t] + cz]);
       }
     };
     A below[CPT], cen[CPT], above[CPT];
@@ -1184,7 +1185,7 @@ __global__ void __launch_bounds__(1024 / CPT + 32)
       own(c + 1, above);
       const B* pk = slot(c % D);
       const int cz = 16 * axis_class(k, NZ);
-      double bd[CPT], bu[CPT], bc[CPT];
+      L bd[CPT], bu[CPT], bc[CPT];
       ldrow(pk + r * NX + i0, bd);
       ldrow(pk + (r + 2) * NX + i0, bu);
       ldrow(pk + (r + 1) * NX + i0, bc);
@@ -1200,13 +1201,14 @@ __global__ void __launch_bounds__(1024 / CPT + 32)
       } else {
 #pragma unroll
         for(int t = 0; t < CPT; ++t) {
-          dn[t] = sd * om * A(bd[t] - sb) * A(invd_s[cdn[t] + cz]);
-          up[t] = su * om * A(bu[t] - sb) * A(invd_s[cup[t] + cz]);
+          dn[t] = sd * om * A(bd[t] - L(sb)) * A(invd_s[cdn[t] + cz]);
+          up[t] = su * om * A(bu[t] - L(sb)) * A(invd_s[cup[t] + cz]);
         }
-        left = A(sxl) * om * A(double(pk[(r + 1) * NX + xl]) - sb) * A(invd_s[cl + cz]);
-        right = A(sxr) * om * A(double(pk[(r + 1) * NX + xr]) - sb) * A(invd_s[cr + cz]);
+        left = A(sxl) * om * A(L(pk[(r + 1) * NX + xl]) - L(sb)) * A(invd_s[cl + cz]);
+        right = A(sxr) * om * A(L(pk[(r + 1) * NX + xr]) - L(sb)) * A(invd_s[cr + cz]);
       }
       A v[CPT];
+      A ps0 = A(0);  // FP32: per-plane partial sum
       const A w0 = om * A(invd_s[0]);
 #pragma unroll
       for(int t = 0; t < CPT; ++t) {
@@ -1216,13 +1218,15 @@ __global__ void __launch_bounds__(1024 / CPT + 32)
         const A ax = -(rr - two_c + l) * ix - (up[t] - two_c + dn[t]) * iy - (above[t] - two_c + below[t]) * iz;
         if constexpr(PER) {
           // a = w (b - sb) on every point, so A a = w A b
-          const A bcs = A(bc[t] - sb);
+          const A bcs = A(bc[t] - L(sb));
           v[t] = w0 * bcs + w0 * (bcs - w0 * ax);
         } else {
-          v[t] = cen[t] + om * (A(bc[t] - sb) - ax) * A(invd_s[cown[t] + cz]);
+          v[t] = cen[t] + om * (A(bc[t] - L(sb)) - ax) * A(invd_s[cown[t] + cz]);
         }
-        acc[0] += double(v[t]);
+        if constexpr(std::is_same_v<T, float>) ps0 += v[t];
+        else acc[0] += double(v[t]);
       }
+      if constexpr(std::is_same_v<T, float>) acc[0] += double(ps0);
       if constexpr(CPT == 4) {
         tstore4<T>(out + o.L.idx(i0, j, k), v);
       } else if constexpr(std::is_same_v<T, double>) {
@@ -1262,7 +1266,8 @@ __global__ void __launch_bounds__(1024 / CPT)
   using A = T;
   extern __shared__ __align__(128) unsigned char tsm[];
   __shared__ uint64_t bars[D];
-  __shared__ double invd_s[64];
+  __shared__ A invd_s[64];
+  using L = std::conditional_t<std::is_same_v<T, float>, float, double>;  // loaded rhs values
   const int NX = o.L.nx, NY = o.L.ny, NZ = o.L.nz;
   const int NXc = NX / 2, NZc = NZ / 2;
   const int TY = 1024 / NX;
@@ -1307,7 +1312,7 @@ __global__ void __launch_bounds__(1024 / CPT)
     for(int sl = 0; sl < D; ++sl) tma::mbar_init(&bars[sl], 1);
     tma::fence_barrier_init();
   }
-  if(threadIdx.x < 64) invd_s[threadIdx.x] = o.invd[threadIdx.x];
+  if(threadIdx.x < 64) invd_s[threadIdx.x] = A(o.invd[threadIdx.x]);
   __syncthreads();
   int next = 0;
   if(threadIdx.x == 0)
@@ -1391,10 +1396,11 @@ __global__ void __launch_bounds__(1024 / CPT)
         left *= A(sxl);
         right *= A(sxr);
       }
-      double bq[CPT];
-      tload4<double>(bk + r * NX + i0, bq);
+      L bq[CPT];
+      tload4<L>(bk + r * NX + i0, bq);
       const int cz = 16 * axis_class(k, NZ);
       A v[CPT];
+      A ps0 = A(0);  // FP32: per-plane partial sum
 #pragma unroll
       for(int t = 0; t < CPT; ++t) {
         const A l = t > 0 ? cen[t - 1] : left;
@@ -1402,11 +1408,13 @@ __global__ void __launch_bounds__(1024 / CPT)
         const A two_c = A(2) * cen[t];
         const A ax = -(rr - two_c + l) * ix - (up[t] - two_c + dn[t]) * iy - (above[t] - two_c + below[t]) * iz;
         if constexpr(PER)
-          v[t] = (cen[t] - sin - sec) + om * (A(bq[t] - sb) - ax) * A(invd_s[0]);
+          v[t] = (cen[t] - sin - sec) + om * (A(bq[t] - L(sb)) - ax) * A(invd_s[0]);
         else
-          v[t] = cen[t] + om * (A(bq[t] - sb) - ax) * A(invd_s[cls[t] + cz]);
-        acc[0] += double(v[t]);
+          v[t] = cen[t] + om * (A(bq[t] - L(sb)) - ax) * A(invd_s[cls[t] + cz]);
+        if constexpr(std::is_same_v<T, float>) ps0 += v[t];
+        else acc[0] += double(v[t]);
       }
+      if constexpr(std::is_same_v<T, float>) acc[0] += double(ps0);
       tstore4<T>(out + o.L.idx(i0, j, k), v);
 #pragma unroll
       for(int t = 0; t < CPT; ++t) {
