@@ -220,7 +220,7 @@ __device__ __forceinline__ void reduce_finish(double (&v)[K], const bool (&is_ma
     // visible (the CTA barrier below passes that on to the block's threads,
     // which read the partials from L2); cheaper than a full fence pair
     unsigned int t;
-    asm volatile("atom.add.acq_rel.gpu.u32 %0, [%1], 1;" : "=r"(t) : "l"(rb.ticket) : "memory");
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;" : "=r"(t) : "l"(rb.ticket) : "memory");
     last = (t == static_cast<unsigned int>(nblocks - 1));
   }
   __syncthreads();
